@@ -1,0 +1,333 @@
+"""Benchmark of the batched phonon NEGF path on B200.
+
+Workload (one step): the quasi-2D slab -- principal layer of 16 atoms x 3 DOF
+(n = 48, complex128), seeded NN+NNN spring network, 64 shifted k-points,
+2048 omegas up to 1.05 omega_max, eta = 1e-6 omega_max^2, 20 identical device
+layers: 131,072 (omega, k) points, each a Sancho-Rubio surface GF plus an RGF
+device solve and the transmission trace, in FP64.  With N ranks each rank
+takes its own 2048-omega shard of an N*2048-omega grid (weak scaling, no
+data-path collective).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Prints one JSON line (rank 0).  ``--impl reference`` times negfpy's CPU
+algorithm (the oracle restatement in oracle/, one process per host core,
+one BLAS thread each) on a bounded sample of the same workload.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+N_OMEGA, N_K, N_LAYERS = 2048, 64, 20
+METRIC = "(omega,k)-points/s, FP64 transmission (SGF + RGF + trace), quasi-2D slab n=48"
+
+
+def _args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="native", choices=["native", "reference"])
+    ap.add_argument("--cpu-sample", type=int, default=0, help="points in the CPU baseline sample (0 = auto)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    return ap.parse_args()
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def _workload(rank: int, world: int):
+    from negfpy_b200 import workloads as W
+
+    wl = W.slab_workload(n_omega=N_OMEGA * world, n_k=N_K, n_layers=N_LAYERS)
+    shard = np.arange(rank, N_OMEGA * world, world)
+    return wl, shard
+
+
+def _config(ws: int) -> dict:
+    return {"workload": f"slab_n48_L{N_LAYERS}_K{N_K}_W{N_OMEGA} per rank", "n": 48, "n_layers": N_LAYERS,
+            "n_k": N_K, "n_omega_per_rank": N_OMEGA, "points_per_rank_per_step": N_OMEGA * N_K,
+            "eta": "1e-6 omega_max^2", "parallelism": f"omega-sharded x{ws}",
+            "l2": "flushed between timed steps (256 MB write)",
+            "leads": "identical left/right lead: one decimation per point"}
+
+
+def _cpu_sample_pairs(wl, shard, n_points, seed=5):
+    rng = np.random.default_rng(seed)
+    wi = rng.choice(shard, size=n_points, replace=True)
+    ki = rng.integers(0, len(wl.kpoints), size=n_points)
+    return [(int(a), int(b)) for a, b in zip(wi, ki)]
+
+
+def cpu_rate(wl, shard, n_points, cores):
+    """Oracle (negfpy's algorithm, SuperLU device solve) on a bounded sample; points/s."""
+    from oracle import negf_oracle as O
+
+    pairs = _cpu_sample_pairs(wl, shard, n_points)
+    t0 = time.perf_counter()
+    O.transmission_points(wl, pairs, processes=cores)
+    dt = time.perf_counter() - t0
+    return n_points / dt, dt
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["clock sampling unavailable"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def fp64_peak_tflops(torch):
+    """Measured FP64 dense throughput on this GPU: cuBLAS DGEMM 8192^3 via torch.matmul, best of 5."""
+    a = torch.randn(8192, 8192, dtype=torch.float64, device="cuda")
+    b = torch.randn(8192, 8192, dtype=torch.float64, device="cuda")
+    torch.matmul(a, b)
+    best = 1e30
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1) / 1e3)
+    del a, b
+    torch.cuda.empty_cache()
+    return 2.0 * 8192 ** 3 / best / 1e12
+
+
+def run_reference(args):
+    ws, rank, _ = _dist()
+    if rank != 0:
+        return
+    cores = os.cpu_count() or 1
+    wl, shard = _workload(0, 1)
+    n = args.cpu_sample or max(4 * cores, 64)
+    if args.warmup > 0:  # one short untimed round starts the worker processes' imports
+        cpu_rate(wl, shard, min(n, 2 * cores), cores)
+    rates = []
+    for s in range(args.steps):
+        r, dt = cpu_rate(wl, shard, n, cores)
+        rates.append(r)
+    v = float(np.mean(rates))
+    out = {
+        "metric": METRIC, "value": v, "unit": "points/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * N_OMEGA * N_K / v, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "complex128", "data": "synthetic", "impl": "reference",
+        "config": dict(_config(ws), sample_points_per_step=n),
+        "cpu_baseline": {"value": v, "unit": "points/s", "cores": cores, "kind": "port",
+                         "sample": f"{n} random (omega,k) points of the {N_OMEGA}x{N_K} slab grid per step; "
+                                   "negfpy's algorithm restated in oracle/ (numpy inv + SuperLU), "
+                                   f"{cores} spawn processes x 1 BLAS thread"},
+        "e2e": {"value": v, "unit": "points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    args = _args()
+    if args.impl == "reference":
+        return run_reference(args)
+    import torch
+    import torch.distributed as dist
+
+    ws, rank, local = _dist()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+    import negfpy_b200 as nb
+    from negfpy_b200 import engine, spectrum
+
+    dev = torch.device("cuda", local)
+    wl, shard = _workload(rank, ws)
+    s = engine.StackedSystem.from_arrays(wl.lead_l, wl.lead_l, wl.onsite, wl.coupling, wl.n_layers)
+    K = len(wl.kpoints)
+    W = len(shard)
+    P = W * K
+    om_all = torch.tensor(wl.omegas[shard], dtype=torch.float64, device=dev)
+    w_idx, k_idx = spectrum.grid_points(W, K, dev)
+    om = om_all[w_idx].contiguous()
+    eta = torch.full_like(om, wl.eta)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # > L2 (126 MB)
+
+    def step(events=None):
+        if events is not None:
+            events[0].record()
+        rl = engine.sgf_sr(*s.lead_l, om, eta, k_idx)
+        if events is not None:
+            events[1].record()
+        T, st = engine.rgf_transmission(s.onsite, s.coupling, s.n_layers, s.vl, s.vr, rl["g"], rl["g"], om, eta,
+                                        k_idx, rl["status"])
+        if events is not None:
+            events[2].record()
+        return rl, T, st
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+    if ws > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        for i in range(args.steps):
+            flush.zero_()  # L2 flush between timed steps, outside the events
+            rl, T, st = step(ev[i])
+        torch.cuda.synchronize()
+    if ws > 1:
+        dist.barrier()
+    t_sr = sum(e[0].elapsed_time(e[1]) for e in ev) / 1e3
+    t_rgf = sum(e[1].elapsed_time(e[2]) for e in ev) / 1e3
+    total = t_sr + t_rgf
+    tmax = torch.tensor([total, t_sr, t_rgf], dtype=torch.float64, device=dev)
+    if ws > 1:
+        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+    total, t_sr, t_rgf = (float(x) for x in tmax.cpu())
+    value = ws * P * args.steps / total
+
+    status = st.cpu().numpy()
+    iters = rl["iters"].cpu().numpy().astype(np.float64)
+    n = wl.n
+    L = wl.n_layers
+    # Algorithmic complex flops (8 real flops per complex multiply-add):
+    # SGF per point: iters*(inverse 8n^3 + 6 products 48n^3) + final inverse 8n^3
+    # RGF per point: Sigma (2 sides x 2 products) 32n^3, layer 0 inverse 8n^3,
+    #   (L-1) x (4 products + inverse) 40n^3, trace 2 products 16n^3
+    f_sr = float(np.sum(iters * 56.0 + 8.0)) * n ** 3
+    f_rgf = P * (32.0 + 8.0 + (L - 1) * 40.0 + 16.0) * n ** 3
+    peak = fp64_peak_tflops(torch)
+    ach_sr = f_sr * args.steps / t_sr / 1e12
+    ach_rgf = f_rgf * args.steps / t_rgf / 1e12
+    dom = "sgf_sr" if t_sr >= t_rgf else "rgf"
+    ach = ach_sr if dom == "sgf_sr" else ach_rgf
+    roof = {"bound": "tensor", "achieved": ach, "peak": peak, "unit": "TFLOP/s", "frac": ach / peak,
+            "traffic": None, "kernel": dom,
+            "peak_source": "measured in this run: FP64 cuBLAS DGEMM 8192^3 via torch.matmul (best of 5); "
+                           "MEASURED_PEAKS.json has no FP64 figure",
+            "kernels": {"sgf_sr": {"tflops": ach_sr, "frac": ach_sr / peak, "s_per_step": t_sr / args.steps,
+                                   "flop_per_step": f_sr},
+                        "rgf": {"tflops": ach_rgf, "frac": ach_rgf / peak, "s_per_step": t_rgf / args.steps,
+                                "flop_per_step": f_rgf}},
+            "mean_sgf_iterations": float(iters.mean())}
+    tr_file = ROOT / "profiles" / "traffic.json"
+    if tr_file.exists():
+        tr = json.loads(tr_file.read_text())
+        roof["traffic"] = tr.get(dom)
+
+    # End to end through the public API: per-k block construction on the host,
+    # upload, GPU solve, result back to host.
+    from negfpy_b200.models import material_kspace_device, material_kspace_lead
+    from negfpy_b200 import workloads as Wm
+
+    params = Wm.spring_network(wl.meta["seed"], ny=wl.meta["ny"], nz=wl.meta["nz"], periodic_y=True)
+    lead_k = material_kspace_lead(params)
+    dev_k = material_kspace_device(L, params)
+    e2e_times = []
+    for _ in range(max(args.e2e_steps, 1)):
+        if ws > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        res = nb.transmission_grid(wl.omegas[shard], wl.kpoints, dev_k, lead_k, lead_k, eta=wl.eta)
+        e2e_times.append(time.perf_counter() - t0)
+    te = torch.tensor([float(np.mean(e2e_times))], dtype=torch.float64, device=dev)
+    if ws > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_val = ws * P / float(te.item())
+    nl = n
+    h2d = (3 * K * nl * nl + K * n * n * 2 + 2 * K * n * nl) * 16 + P * (8 + 8 + 8 + 4)
+    d2h = P * (8 + 4 + 4 + 4)
+    e2e_diff = float(np.max(np.abs(res["T"].ravel() - T.cpu().numpy()) / np.maximum(np.abs(T.cpu().numpy()), 1)))
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        cores = os.cpu_count() or 1
+        nsamp = args.cpu_sample or max(8 * cores, 64)
+        rate, dt = cpu_rate(wl, shard, nsamp, cores)
+        cpu = {"value": rate, "unit": "points/s", "cores": cores, "kind": "port",
+               "sample": f"{nsamp} random points of the {W}x{K} grid ({dt:.1f} s wall); negfpy's algorithm "
+                         "restated in oracle/ (numpy inv + SuperLU), spawn pool, 1 BLAS thread per process"}
+
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": value, "unit": "points/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "complex128", "data": "synthetic",
+            "config": _config(ws),
+            "roofline": roof,
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_val, "unit": "points/s", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h), "api": "negfpy_b200.transmission_grid (LeadKSpace/DeviceKSpace)",
+                    "max_rel_diff_vs_device_run": e2e_diff},
+            "gpu_launches": 2 * args.steps,
+            "status_ok_fraction": float(np.mean(status == 0)),
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(out), flush=True)
+    if ws > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

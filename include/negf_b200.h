@@ -1,0 +1,118 @@
+/*
+ * negf_b200.h -- C ABI of libnegfb200.so, the B200 kernels of the
+ * per-(omega, k) phonon NEGF path.
+ *
+ * Conventions
+ *  - All array pointers are DEVICE pointers owned by the caller.
+ *  - Complex matrices are interleaved (re, im) float64 pairs, row-major.
+ *    Strides are counted in complex elements.
+ *  - `stream` is a cudaStream_t (NULL = legacy default stream).  Calls are
+ *    asynchronous on that stream; nothing is allocated by the library
+ *    (the caller provides every workspace) and nothing is synchronised.
+ *  - Return value: 0 on success, negative on a launch-level problem
+ *    (NEGF_EINVAL bad argument, NEGF_EUNSUPPORTED size not built,
+ *    NEGF_ECUDA CUDA error); negf_last_error() describes it.  Numerical
+ *    outcomes are per point in `status_out`: NEGF_OK, NEGF_MAXITER,
+ *    NEGF_NONFINITE, NEGF_SINGULAR, NEGF_REFINE_FAIL.
+ *
+ * Each entry point names the negfpy routine it replaces (paths relative to
+ * the negfpy project root).
+ */
+#ifndef NEGF_B200_H
+#define NEGF_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NEGF_B200_ABI_VERSION 1
+
+#define NEGF_OK 0
+#define NEGF_MAXITER 1
+#define NEGF_NONFINITE 2
+#define NEGF_SINGULAR 3
+#define NEGF_REFINE_FAIL 4
+
+#define NEGF_EINVAL (-1)
+#define NEGF_EUNSUPPORTED (-2)
+#define NEGF_ECUDA (-3)
+
+/* ABI version (NEGF_B200_ABI_VERSION). */
+int negf_get_version(void);
+
+/* Description of the last failing call on this host thread. */
+const char* negf_last_error(void);
+
+/* Largest block order the FP64 kernels accept. */
+int negf_max_order_f64(void);
+
+/*
+ * Batched Sancho-Rubio surface Green's function, FP64.
+ * Replaces negfpy core/surface_gf.py:18-81 (surface_gf_sancho_rubio, reached
+ * through the dispatcher core/surface_gf.py:254-311 with method
+ * "sancho_rubio") and, through dos_out, the trace of core/dos.py:31-61.
+ *
+ * Point p uses lead set k = k_index[p] (k_index NULL: k = 0), whose blocks
+ * are h00/h01/h10 + k*lead_stride (n x n each; h10 NULL means h01^H), and
+ * z = (omega[p] + i eta[p])^2.  Outputs (each may be NULL):
+ *   g_out[p]      n x n surface Green's function
+ *   dos_out[p]    (omega/pi) Re Tr[i (g - g^H)]
+ *   iters_out[p]  decimation sweeps taken
+ *   status_out[p] NEGF_OK / NEGF_MAXITER / NEGF_NONFINITE / NEGF_SINGULAR
+ */
+int negf_sgf_sr_f64(int n, int batch, const double* h00, const double* h01, const double* h10,
+                    long long lead_stride, const int* k_index, const double* omega, const double* eta,
+                    double tol, int maxiter, double* g_out, double* dos_out, int* iters_out, int* status_out,
+                    void* stream);
+
+/* Workspace bytes negf_rgf_transmission_f64 needs (0 on a bad size). */
+size_t negf_rgf_workspace_bytes(int n_dev, int n_lead_l, int n_lead_r);
+
+/*
+ * Batched device solve and transmission, FP64.
+ * Replaces negfpy core/negf.py:306-357 (transmission) including
+ * core/negf.py:141-250 (system assembly, Sigma = V g V^H at :72-97) and the
+ * SuperLU solve at :353, by a recursive Green's function sweep.
+ *
+ * Point p uses k = k_index[p]; onsite block l is onsite + k*onsite_kstride +
+ * l*onsite_lstride, coupling block l (between layers l, l+1; its conjugate
+ * transpose sits below the diagonal) is coupling + k*coupling_kstride +
+ * l*coupling_lstride.  v_left (n_dev x n_lead_l) and v_right
+ * (n_dev x n_lead_r) are the device-to-lead couplings with the contact DOFs
+ * of the first / last layer as rows (zero rows elsewhere); their k stride
+ * may be 0.  g_left/g_right are per-point surface Green's functions (point
+ * stride g_*_pstride; g_right may equal g_left).  lead_status (may be NULL)
+ * skips points whose surface GF failed, copying the status.
+ * Output: t_out[p] = Re Tr[Gamma_L G_LR Gamma_R G_LR^H] (NaN on failure).
+ */
+int negf_rgf_transmission_f64(int n_dev, int n_lead_l, int n_lead_r, int n_layers, int batch,
+                              const double* onsite, long long onsite_kstride, long long onsite_lstride,
+                              const double* coupling, long long coupling_kstride, long long coupling_lstride,
+                              const double* v_left, long long v_left_kstride, const double* v_right,
+                              long long v_right_kstride, const double* g_left, long long g_left_pstride,
+                              const double* g_right, long long g_right_pstride, const int* k_index,
+                              const double* omega, const double* eta_device, const int* lead_status,
+                              double* t_out, int* status_out, void* workspace, size_t workspace_bytes,
+                              void* stream);
+
+/*
+ * k average of an omega-major [n_omega][n_k] transmission table.
+ * Replaces the mean in negfpy core/negf.py:360-397 (transmission_kavg).
+ */
+int negf_kavg_f64(const double* t, int n_omega, int n_k, double* t_mean, void* stream);
+
+/*
+ * Thermal conductance kappa(T_j) = (1/2pi) trapz(kB t_mean x^2 e^-x/(1-e^-x)^2, w)
+ * with w = omega * omega_unit_rad_s and x = hbar w / (kB T_j).
+ * Replaces negfpy workflows/ifc_bulk.py:408-438 (_thermal_conductance_from_spectrum).
+ */
+int negf_kappa_f64(const double* omega, const double* t_mean, int n_omega, const double* temperatures, int n_temps,
+                   double omega_unit_rad_s, double* kappa_out, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NEGF_B200_H */

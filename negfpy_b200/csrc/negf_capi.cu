@@ -1,0 +1,155 @@
+// extern "C" entry points of libnegfb200.so (declared in include/negf_b200.h).
+// Argument checks happen here, on the host; the kernels assume valid input.
+#include <cstdio>
+#include <cstring>
+
+#include "../../include/negf_b200.h"
+#include "negf_f64.h"
+
+namespace {
+thread_local char g_err[256] = "";
+
+int fail(int code, const char* msg) {
+  std::snprintf(g_err, sizeof(g_err), "%s", msg);
+  return code;
+}
+int cuda_fail(const char* where) {
+  cudaError_t e = cudaGetLastError();
+  std::snprintf(g_err, sizeof(g_err), "%s: %s", where, cudaGetErrorString(e));
+  return NEGF_ECUDA;
+}
+inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+constexpr size_t kCounterBytes = 256;
+}  // namespace
+
+extern "C" {
+
+int negf_get_version(void) { return NEGF_B200_ABI_VERSION; }
+
+const char* negf_last_error(void) { return g_err; }
+
+int negf_max_order_f64(void) { return 48; }
+
+int negf_sgf_sr_f64(int n, int batch, const double* h00, const double* h01, const double* h10, long long lead_stride,
+                    const int* k_index, const double* omega, const double* eta, double tol, int maxiter,
+                    double* g_out, double* dos_out, int* iters_out, int* status_out, void* stream) {
+  if (n <= 0 || batch < 0) return fail(NEGF_EINVAL, "negf_sgf_sr_f64: n must be positive and batch non-negative");
+  if (!h00 || !h01 || !omega || !eta) return fail(NEGF_EINVAL, "negf_sgf_sr_f64: null input pointer");
+  if (maxiter <= 0 || !(tol > 0.0)) return fail(NEGF_EINVAL, "negf_sgf_sr_f64: maxiter and tol must be positive");
+  if (lead_stride < 0) return fail(NEGF_EINVAL, "negf_sgf_sr_f64: negative lead_stride");
+  if (negf::padded_order(n) == 0) return fail(NEGF_EUNSUPPORTED, "negf_sgf_sr_f64: block order above 48");
+  negf::SrArgs a;
+  a.n = n;
+  a.batch = batch;
+  a.h00 = reinterpret_cast<const double2*>(h00);
+  a.h01 = reinterpret_cast<const double2*>(h01);
+  a.h10 = reinterpret_cast<const double2*>(h10);
+  a.lead_stride = lead_stride;
+  a.kidx = k_index;
+  a.omega = omega;
+  a.eta = eta;
+  a.tol = tol;
+  a.maxiter = maxiter;
+  a.g_out = reinterpret_cast<double2*>(g_out);
+  a.dos_out = dos_out;
+  a.iters_out = iters_out;
+  a.status_out = status_out;
+  int rc = negf::sr_f64_launch(a, as_stream(stream));
+  if (rc == -2) return fail(NEGF_EUNSUPPORTED, "negf_sgf_sr_f64: block order not built");
+  if (rc != 0) return cuda_fail("negf_sgf_sr_f64");
+  return 0;
+}
+
+namespace {
+int max3(int a, int b, int c) { return a > b ? (a > c ? a : c) : (b > c ? b : c); }
+// Persistent grid of the RGF kernel (0 for the 1x1 path, negative on error).
+int rgf_grid_for(int np) { return np == 1 ? 0 : negf::rgf_f64_grid(np); }
+}  // namespace
+
+size_t negf_rgf_workspace_bytes(int n_dev, int n_lead_l, int n_lead_r) {
+  if (n_dev <= 0 || n_lead_l <= 0 || n_lead_r <= 0) return 0;
+  const int np = negf::padded_order(max3(n_dev, n_lead_l, n_lead_r));
+  if (np == 0) return 0;
+  const int grid = rgf_grid_for(np);
+  if (grid < 0) return 0;
+  return kCounterBytes + (size_t)grid * 2 * n_dev * n_dev * 16;
+}
+
+int negf_rgf_transmission_f64(int n_dev, int n_lead_l, int n_lead_r, int n_layers, int batch, const double* onsite,
+                              long long onsite_kstride, long long onsite_lstride, const double* coupling,
+                              long long coupling_kstride, long long coupling_lstride, const double* v_left,
+                              long long v_left_kstride, const double* v_right, long long v_right_kstride,
+                              const double* g_left, long long g_left_pstride, const double* g_right,
+                              long long g_right_pstride, const int* k_index, const double* omega,
+                              const double* eta_device, const int* lead_status, double* t_out, int* status_out,
+                              void* workspace, size_t workspace_bytes, void* stream) {
+  if (n_dev <= 0 || n_lead_l <= 0 || n_lead_r <= 0 || n_layers <= 0 || batch < 0)
+    return fail(NEGF_EINVAL, "negf_rgf_transmission_f64: sizes must be positive");
+  if (!onsite || !v_left || !v_right || !g_left || !g_right || !omega || !eta_device || !t_out)
+    return fail(NEGF_EINVAL, "negf_rgf_transmission_f64: null pointer");
+  if (n_layers > 1 && !coupling) return fail(NEGF_EINVAL, "negf_rgf_transmission_f64: null coupling");
+  if (onsite_kstride < 0 || onsite_lstride < 0 || coupling_kstride < 0 || coupling_lstride < 0 ||
+      v_left_kstride < 0 || v_right_kstride < 0 || g_left_pstride < 0 || g_right_pstride < 0)
+    return fail(NEGF_EINVAL, "negf_rgf_transmission_f64: negative stride");
+  const int np = negf::padded_order(max3(n_dev, n_lead_l, n_lead_r));
+  if (np == 0) return fail(NEGF_EUNSUPPORTED, "negf_rgf_transmission_f64: block order above 48");
+  const int grid = rgf_grid_for(np);
+  if (grid < 0) return cuda_fail("negf_rgf_transmission_f64: occupancy query");
+  const size_t need = kCounterBytes + (size_t)grid * 2 * n_dev * n_dev * 16;
+  if (!workspace || workspace_bytes < need)
+    return fail(NEGF_EINVAL, "negf_rgf_transmission_f64: workspace missing or too small");
+  if (batch == 0) return 0;
+  negf::RgfArgs a;
+  a.n = n_dev;
+  a.nl = n_lead_l;
+  a.nr = n_lead_r;
+  a.L = n_layers;
+  a.batch = batch;
+  a.D = reinterpret_cast<const double2*>(onsite);
+  a.d_ks = onsite_kstride;
+  a.d_ls = onsite_lstride;
+  a.C = reinterpret_cast<const double2*>(coupling ? coupling : onsite);
+  a.c_ks = coupling_kstride;
+  a.c_ls = coupling_lstride;
+  a.VL = reinterpret_cast<const double2*>(v_left);
+  a.vl_ks = v_left_kstride;
+  a.VR = reinterpret_cast<const double2*>(v_right);
+  a.vr_ks = v_right_kstride;
+  a.gL = reinterpret_cast<const double2*>(g_left);
+  a.gl_ps = g_left_pstride;
+  a.gR = reinterpret_cast<const double2*>(g_right);
+  a.gr_ps = g_right_pstride;
+  a.kidx = k_index;
+  a.omega = omega;
+  a.eta_dev = eta_device;
+  a.lead_status = lead_status;
+  a.T_out = t_out;
+  a.status_out = status_out;
+  a.counter = reinterpret_cast<unsigned int*>(workspace);
+  a.sigma_ws = reinterpret_cast<double2*>(static_cast<char*>(workspace) + kCounterBytes);
+  cudaStream_t st = as_stream(stream);
+  if (np != 1 && cudaMemsetAsync(workspace, 0, sizeof(unsigned int), st) != cudaSuccess)
+    return cuda_fail("negf_rgf_transmission_f64: counter reset");
+  int rc = negf::rgf_f64_launch(a, np, grid, st);
+  if (rc == -2) return fail(NEGF_EUNSUPPORTED, "negf_rgf_transmission_f64: block order not built");
+  if (rc != 0) return cuda_fail("negf_rgf_transmission_f64");
+  return 0;
+}
+
+int negf_kavg_f64(const double* t, int n_omega, int n_k, double* t_mean, void* stream) {
+  if (n_omega < 0 || n_k <= 0 || !t || !t_mean) return fail(NEGF_EINVAL, "negf_kavg_f64: bad argument");
+  if (negf::kavg_launch(t, n_omega, n_k, t_mean, as_stream(stream)) != 0) return cuda_fail("negf_kavg_f64");
+  return 0;
+}
+
+int negf_kappa_f64(const double* omega, const double* t_mean, int n_omega, const double* temperatures, int n_temps,
+                   double omega_unit_rad_s, double* kappa_out, void* stream) {
+  if (n_omega < 2 || n_temps < 0 || !omega || !t_mean || !temperatures || !kappa_out)
+    return fail(NEGF_EINVAL, "negf_kappa_f64: bad argument");
+  if (negf::kappa_launch(omega, t_mean, n_omega, temperatures, n_temps, omega_unit_rad_s, kappa_out,
+                         as_stream(stream)) != 0)
+    return cuda_fail("negf_kappa_f64");
+  return 0;
+}
+
+}  // extern "C"

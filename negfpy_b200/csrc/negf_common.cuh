@@ -1,0 +1,101 @@
+// Device helpers shared by the NEGF kernels: complex arithmetic on
+// interleaved (re, im) pairs, block reductions, and the per-point status codes.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace negf {
+
+// Per-point numerical status (also the values of the C-ABI status arrays).
+enum Status : int {
+  kOk = 0,
+  kMaxIter = 1,     // Sancho-Rubio did not reach tol within maxiter
+  kNonFinite = 2,   // inf/nan appeared
+  kSingular = 3,    // exact zero pivot in an inversion
+  kRefineFail = 4,  // mixed-precision refinement did not converge
+};
+
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double2 cneg(double2 a) { return make_double2(-a.x, -a.y); }
+__device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
+}
+// acc += a * b, four FP64 FMAs.
+__device__ __forceinline__ void cfma(double2& acc, double2 a, double2 b) {
+  acc.x = fma(a.x, b.x, acc.x);
+  acc.x = fma(-a.y, b.y, acc.x);
+  acc.y = fma(a.x, b.y, acc.y);
+  acc.y = fma(a.y, b.x, acc.y);
+}
+// 1 / (a + ib) by Smith's algorithm (R. L. Smith, CACM 5(8), 1962), which
+// scales by the larger component to avoid overflow in a^2 + b^2.
+__device__ __forceinline__ double2 crecip(double2 v) {
+  double a = v.x, b = v.y;
+  if (fabs(a) >= fabs(b)) {
+    double r = b / a;
+    double d = a + b * r;
+    return make_double2(1.0 / d, -r / d);
+  } else {
+    double r = a / b;
+    double d = a * r + b;
+    return make_double2(r / d, -1.0 / d);
+  }
+}
+__device__ __forceinline__ double cabs1(double2 a) { return fabs(a.x) + fabs(a.y); }
+__device__ __forceinline__ double cabs2(double2 a) { return a.x * a.x + a.y * a.y; }
+__device__ __forceinline__ bool cfinite(double2 a) { return isfinite(a.x) && isfinite(a.y); }
+
+// Single precision counterparts for the mixed-precision kernels.
+__device__ __forceinline__ void cfma(float2& acc, float2 a, float2 b) {
+  acc.x = fmaf(a.x, b.x, acc.x);
+  acc.x = fmaf(-a.y, b.y, acc.x);
+  acc.y = fmaf(a.x, b.y, acc.y);
+  acc.y = fmaf(a.y, b.x, acc.y);
+}
+
+// Block-wide reductions.  `red` must hold at least 33 doubles of shared
+// memory; every thread of the block must call with uniform control flow.
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ double block_max(double v, double* red) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  v = warp_max(v);
+  __syncthreads();  // protects `red` from a previous reduction still being read
+  if (lane == 0) red[wid] = v;
+  __syncthreads();
+  if (wid == 0) {
+    double w = lane < nw ? red[lane] : -1.0;
+    w = warp_max(w);
+    if (lane == 0) red[32] = w;
+  }
+  __syncthreads();
+  return red[32];
+}
+__device__ __forceinline__ double block_sum(double v, double* red) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  v = warp_sum(v);
+  __syncthreads();
+  if (lane == 0) red[wid] = v;
+  __syncthreads();
+  if (wid == 0) {
+    double w = lane < nw ? red[lane] : 0.0;
+    w = warp_sum(w);
+    if (lane == 0) red[32] = w;
+  }
+  __syncthreads();
+  return red[32];
+}
+// Returns nonzero in every thread if any thread passed nonzero.
+__device__ __forceinline__ int block_any(int v) { return __syncthreads_or(v); }
+
+}  // namespace negf

@@ -1,0 +1,54 @@
+// Internal launch interface of the FP64 kernels (not part of the C-ABI).
+#pragma once
+#include <cuda_runtime.h>
+
+namespace negf {
+
+// Sancho-Rubio over a batch of points; complex matrices are interleaved
+// (re, im) double pairs, row-major, order n.
+struct SrArgs {
+  int n, batch;
+  const double2* h00;
+  const double2* h01;
+  const double2* h10;      // nullptr: d10 = d01^H
+  long long lead_stride;   // complex elements between consecutive lead sets
+  const int* kidx;         // [batch] lead-set index per point (nullptr: set 0)
+  const double* omega;     // [batch]
+  const double* eta;       // [batch]
+  double tol;
+  int maxiter;
+  double2* g_out;          // [batch][n][n] or nullptr
+  double* dos_out;         // [batch] or nullptr
+  int* iters_out;          // [batch] or nullptr
+  int* status_out;         // [batch] or nullptr
+};
+
+// Device solve + transmission over a batch of points.
+struct RgfArgs {
+  int n, nl, nr, L, batch;
+  const double2* D;  long long d_ks, d_ls;    // onsite block (k, l) at D + k*d_ks + l*d_ls
+  const double2* C;  long long c_ks, c_ls;    // coupling block (k, l) between layers l and l+1
+  const double2* VL; long long vl_ks;         // [.][n][nl] device-to-left-lead coupling
+  const double2* VR; long long vr_ks;         // [.][n][nr]
+  const double2* gL; long long gl_ps;         // per-point left surface GF, stride per point
+  const double2* gR; long long gr_ps;
+  const int* kidx;
+  const double* omega;
+  const double* eta_dev;
+  const int* lead_status;   // [batch] or nullptr; nonzero skips the point
+  double* T_out;            // [batch]
+  int* status_out;          // [batch] or nullptr
+  double2* sigma_ws;        // [grid][2][n][n] scratch
+  unsigned int* counter;    // zeroed work counter
+};
+
+int padded_order(int n);
+int sr_f64_launch(const SrArgs& a, cudaStream_t st);
+// Padded order np = padded_order(max(n, nl, nr)) selects the kernel variant.
+int rgf_f64_grid(int np);  // persistent grid size (blocks), 0 for the 1x1 path
+int rgf_f64_launch(const RgfArgs& a, int np, int grid, cudaStream_t st);
+int kavg_launch(const double* T, int W, int K, double* tbar, cudaStream_t st);
+int kappa_launch(const double* om, const double* tbar, int W, const double* temps, int nT, double unit, double* out,
+                 cudaStream_t st);
+
+}  // namespace negf

@@ -1,0 +1,226 @@
+"""Batched device-side engine: stacked blocks on the GPU, one launch per stage.
+
+A *point* is one (omega, k) pair.  Blocks are stacked per k once
+(``[K, n, n]`` for lead blocks, ``[K, L or 1, n, n]`` for the device) and
+every point carries its k index, so a frequency sweep never rebuilds or
+re-uploads blocks.  Stages per chunk of points:
+
+1. ``negf_sgf_sr_f64`` for the left lead (and the right lead unless both
+   leads are the same object, in which case its result is reused),
+2. ``negf_rgf_transmission_f64`` for Sigma, the RGF sweep and the trace.
+
+All tensors are complex128/float64 on the current CUDA device.
+"""
+
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import _lib
+
+CDT = torch.complex128
+RDT = torch.float64
+
+
+def _dev() -> torch.device:
+    return _lib.require_cuda()
+
+
+def _c(t, device=None) -> torch.Tensor:
+    t = torch.as_tensor(np.asarray(t) if not isinstance(t, torch.Tensor) else t)
+    return t.to(device=device or _dev(), dtype=CDT).contiguous()
+
+
+def _r(t, device=None) -> torch.Tensor:
+    t = torch.as_tensor(t) if not isinstance(t, torch.Tensor) else t
+    return t.to(device=device or _dev(), dtype=RDT).contiguous()
+
+
+def sgf_sr(d00: torch.Tensor, d01: torch.Tensor, d10: torch.Tensor | None, omega: torch.Tensor, eta: torch.Tensor,
+           k_index: torch.Tensor | None = None, tol: float = 1e-12, maxiter: int = 200, want_g: bool = True,
+           want_dos: bool = False, stream=None) -> dict:
+    """Sancho-Rubio surface GF for P points over K stacked lead sets ``[K, n, n]``."""
+    lib = _lib.load()
+    dev = _dev()
+    if d00.dim() == 2:
+        d00, d01 = d00[None], d01[None]
+        d10 = None if d10 is None else d10[None]
+    K, n, _ = d00.shape
+    P = int(omega.shape[0])
+    g = torch.empty((P, n, n), dtype=CDT, device=dev) if want_g else None
+    dos = torch.empty(P, dtype=RDT, device=dev) if want_dos else None
+    iters = torch.empty(P, dtype=torch.int32, device=dev)
+    status = torch.empty(P, dtype=torch.int32, device=dev)
+    if P == 0:
+        return {"g": g, "dos": dos, "iters": iters, "status": status}
+    if k_index is not None:
+        k_index = k_index.to(device=dev, dtype=torch.int32).contiguous()
+    rc = lib.negf_sgf_sr_f64(n, P, _lib.ptr(d00), _lib.ptr(d01), _lib.ptr(d10), n * n if K > 1 else 0,
+                             _lib.ptr(k_index), _lib.ptr(omega), _lib.ptr(eta), float(tol), int(maxiter),
+                             _lib.ptr(g), _lib.ptr(dos), _lib.ptr(iters), _lib.ptr(status),
+                             _lib.stream_handle(stream))
+    _lib.check(rc, "negf_sgf_sr_f64")
+    return {"g": g, "dos": dos, "iters": iters, "status": status}
+
+
+_ws_cache: dict = {}
+
+
+def _workspace(nbytes: int, dev: torch.device) -> torch.Tensor:
+    key = (dev.index,)
+    t = _ws_cache.get(key)
+    if t is None or t.numel() < nbytes:
+        t = torch.empty(max(nbytes, 256), dtype=torch.uint8, device=dev)
+        _ws_cache[key] = t
+    return t
+
+
+def rgf_transmission(onsite: torch.Tensor, coupling: torch.Tensor | None, n_layers: int, vl: torch.Tensor,
+                     vr: torch.Tensor, gl: torch.Tensor, gr: torch.Tensor, omega: torch.Tensor,
+                     eta_dev: torch.Tensor, k_index: torch.Tensor | None, lead_status: torch.Tensor | None,
+                     stream=None) -> tuple[torch.Tensor, torch.Tensor]:
+    """T for P points.  ``onsite`` ``[K, L|1, n, n]``, ``coupling`` ``[K, L-1|1, n, n]``,
+    ``vl`` ``[K|1, n, nl]``, ``vr`` ``[K|1, n, nr]``, ``gl`` ``[P, nl, nl]``, ``gr`` ``[P, nr, nr]``."""
+    lib = _lib.load()
+    dev = _dev()
+    K, Lo, n, _ = onsite.shape
+    nl, nr = int(vl.shape[-1]), int(vr.shape[-1])
+    P = int(omega.shape[0])
+    T = torch.empty(P, dtype=RDT, device=dev)
+    st = torch.empty(P, dtype=torch.int32, device=dev)
+    if P == 0:
+        return T, st
+    on_ks = Lo * n * n if K > 1 else 0
+    on_ls = 0 if Lo == 1 else n * n
+    if coupling is None or n_layers == 1:
+        cp, cp_ks, cp_ls = None, 0, 0
+    else:
+        Kc, Lc = coupling.shape[0], coupling.shape[1]
+        cp, cp_ks, cp_ls = coupling, (Lc * n * n if Kc > 1 else 0), (0 if Lc == 1 else n * n)
+    vl_ks = n * nl if vl.shape[0] > 1 else 0
+    vr_ks = n * nr if vr.shape[0] > 1 else 0
+    need = int(lib.negf_rgf_workspace_bytes(n, nl, nr))
+    if need == 0:
+        raise RuntimeError(f"block order {max(n, nl, nr)} is not supported by the FP64 kernels")
+    ws = _workspace(need, dev)
+    if k_index is not None:
+        k_index = k_index.to(device=dev, dtype=torch.int32).contiguous()
+    rc = lib.negf_rgf_transmission_f64(
+        n, nl, nr, int(n_layers), P, _lib.ptr(onsite), on_ks, on_ls, _lib.ptr(cp), cp_ks, cp_ls, _lib.ptr(vl), vl_ks,
+        _lib.ptr(vr), vr_ks, _lib.ptr(gl), nl * nl, _lib.ptr(gr), nr * nr, _lib.ptr(k_index), _lib.ptr(omega),
+        _lib.ptr(eta_dev), _lib.ptr(lead_status), _lib.ptr(T), _lib.ptr(st), _lib.ptr(ws), ws.numel(),
+        _lib.stream_handle(stream))
+    _lib.check(rc, "negf_rgf_transmission_f64")
+    return T, st
+
+
+def kavg(T_wk: torch.Tensor, stream=None) -> torch.Tensor:
+    """Mean over k of an omega-major ``[W, K]`` table."""
+    lib = _lib.load()
+    W, K = T_wk.shape
+    out = torch.empty(W, dtype=RDT, device=T_wk.device)
+    _lib.check(lib.negf_kavg_f64(_lib.ptr(T_wk.contiguous()), W, K, _lib.ptr(out), _lib.stream_handle(stream)),
+               "negf_kavg_f64")
+    return out
+
+
+def kappa(omega: torch.Tensor, tbar: torch.Tensor, temperatures, omega_unit_rad_s: float, stream=None) -> torch.Tensor:
+    lib = _lib.load()
+    temps = _r(torch.as_tensor(np.atleast_1d(np.asarray(temperatures, dtype=float))), omega.device)
+    out = torch.empty(temps.shape[0], dtype=RDT, device=omega.device)
+    _lib.check(lib.negf_kappa_f64(_lib.ptr(omega), _lib.ptr(tbar), int(omega.shape[0]), _lib.ptr(temps),
+                                  int(temps.shape[0]), float(omega_unit_rad_s), _lib.ptr(out),
+                                  _lib.stream_handle(stream)), "negf_kappa_f64")
+    return out
+
+
+@dataclass
+class StackedSystem:
+    """Device-resident blocks of one lead/device/lead system over K k-points."""
+
+    lead_l: tuple  # (d00, d01, d10|None) [K, nl, nl]
+    lead_r: tuple
+    onsite: torch.Tensor  # [K, L|1, n, n]
+    coupling: torch.Tensor | None  # [K, L-1|1, n, n]
+    n_layers: int
+    vl: torch.Tensor  # [K|1, n, nl]
+    vr: torch.Tensor  # [K|1, n, nr]
+    same_leads: bool
+
+    @property
+    def n(self) -> int:
+        return int(self.onsite.shape[-1])
+
+    @property
+    def K(self) -> int:
+        return int(self.onsite.shape[0])
+
+    @property
+    def nl(self) -> int:
+        return int(self.lead_l[0].shape[-1])
+
+    @property
+    def nr(self) -> int:
+        return int(self.lead_r[0].shape[-1])
+
+    @classmethod
+    def from_arrays(cls, lead_l: dict, lead_r: dict, onsite, coupling, n_layers: int, vl=None, vr=None,
+                    same_leads: bool | None = None) -> "StackedSystem":
+        """Upload host arrays (numpy or torch).  ``vl``/``vr`` default to negfpy's
+        matched-contact couplings V_L = d10 (or d01^H) and V_R = d01 (core/negf.py:192-201),
+        contacting the whole first / last layer."""
+        dev = _dev()
+        ll = (_c(lead_l["d00"], dev), _c(lead_l["d01"], dev),
+              None if lead_l.get("d10") is None else _c(lead_l["d10"], dev))
+        if same_leads is None:
+            same_leads = lead_r is lead_l
+        lr = ll if same_leads else (_c(lead_r["d00"], dev), _c(lead_r["d01"], dev),
+                                    None if lead_r.get("d10") is None else _c(lead_r["d10"], dev))
+        on = _c(onsite, dev)
+        cp = None if coupling is None else _c(coupling, dev)
+        n = on.shape[-1]
+        if vl is None:
+            vl = ll[2] if ll[2] is not None else ll[1].conj().transpose(-1, -2)
+            if vl.shape[-2] != n:
+                raise ValueError("default left coupling needs the device block order to equal the lead's")
+        if vr is None:
+            vr = lr[1]
+            if vr.shape[-2] != n:
+                raise ValueError("default right coupling needs the device block order to equal the lead's")
+        return cls(ll, lr, on, cp, int(n_layers), _c(vl, dev), _c(vr, dev), bool(same_leads))
+
+    def transmission(self, omega: torch.Tensor, k_index: torch.Tensor, eta: torch.Tensor,
+                     eta_dev: torch.Tensor | None = None, tol: float = 1e-12, maxiter: int = 200,
+                     chunk: int = 1 << 15, stream=None) -> dict:
+        """T, status and decimation counts for P points (float64/int32 tensors)."""
+        dev = _dev()
+        P = int(omega.shape[0])
+        omega = _r(omega, dev)
+        eta = _r(eta, dev)
+        eta_dev = eta if eta_dev is None else _r(eta_dev, dev)
+        k_index = k_index.to(device=dev, dtype=torch.int32).contiguous()
+        T = torch.empty(P, dtype=RDT, device=dev)
+        st = torch.empty(P, dtype=torch.int32, device=dev)
+        itl = torch.empty(P, dtype=torch.int32, device=dev)
+        itr = torch.empty(P, dtype=torch.int32, device=dev)
+        for a in range(0, P, chunk):
+            b = min(P, a + chunk)
+            sl = slice(a, b)
+            om, et, ed, ki = omega[sl], eta[sl], eta_dev[sl], k_index[sl]
+            rl = sgf_sr(*self.lead_l, om, et, ki, tol, maxiter, stream=stream)
+            if self.same_leads:
+                rr = rl
+                lst = rl["status"]
+            else:
+                rr = sgf_sr(*self.lead_r, om, et, ki, tol, maxiter, stream=stream)
+                lst = torch.where(rl["status"] != 0, rl["status"], rr["status"])
+            t, s = rgf_transmission(self.onsite, self.coupling, self.n_layers, self.vl, self.vr, rl["g"], rr["g"],
+                                    om, ed, ki, lst, stream=stream)
+            T[sl] = t
+            st[sl] = s
+            itl[sl] = rl["iters"]
+            itr[sl] = rr["iters"]
+        return {"T": T, "status": st, "iters_left": itl, "iters_right": itr}

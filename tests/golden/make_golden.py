@@ -1,0 +1,133 @@
+"""Generate the golden vectors of the NEGF path by running negfpy itself.
+
+Run from the repository root, with negfpy importable (its ``src`` directory on
+PYTHONPATH; the default below is where this build's reference checkout lives):
+
+    python tests/golden/make_golden.py [--ref /path/to/negfpy/src]
+
+Inputs are the seeded synthetic workloads of ``negfpy_b200.workloads`` (their
+blocks are stored with the outputs, so the fixtures do not depend on the
+generator staying bit-stable), plus the small analytic systems of negfpy's
+own test-suite.  Every output here is computed by negfpy's public functions
+(``transmission``, ``surface_gf``, ``lead_surface_dos``, the workflow's
+``_thermal_conductance_from_spectrum``) in FP64 with Sancho-Rubio, and for a
+few points also with the QEP eigen method as an independent cross-check.
+"""
+
+from __future__ import annotations
+
+import argparse
+import sys
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parents[2]
+OUT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ref", default="/root/reference/src")
+    args = ap.parse_args()
+    sys.path.insert(0, args.ref)
+    import negfpy.core as R
+    from negfpy.core.types import Device1D, LeadBlocks
+    from negfpy.models import (ChainParams, MultiDofCellParams, SquareLatticeParams, device_perfect_chain,
+                               lead_blocks, multidof_device, multidof_lead_blocks, square_lattice_device,
+                               square_lattice_lead)
+    from negfpy.modeling.units import qe_omega_to_rad_s
+    from negfpy.workflows.ifc_bulk import _thermal_conductance_from_spectrum
+
+    from negfpy_b200 import workloads as W
+
+    qe_unit = float(qe_omega_to_rad_s(1.0))
+
+    # ---- chain: 1000 omega in (0, 2), L = 8, eta = 1e-8 --------------------
+    wl = W.chain_workload()
+    p = ChainParams(1.0, 1.0)
+    lead = lead_blocks(p)
+    dev = device_perfect_chain(8, p)
+    t_chain = np.array([R.transmission(float(w), dev, lead, lead, eta=1e-8) for w in wl.omegas])
+    g_chain = np.array([R.surface_gf(float(w), lead.d00, lead.d01, eta=1e-8)[0, 0] for w in wl.omegas[::50]])
+    dos_chain = np.array([R.lead_surface_dos(float(w), lead, eta=1e-8) for w in wl.omegas[::50]])
+    temps = np.array([50.0, 300.0, 1000.0])
+    kappa_chain = _thermal_conductance_from_spectrum(wl.omegas * wl.omega_unit_rad_s / qe_unit, t_chain, temps)
+    np.savez_compressed(OUT / "chain.npz", omegas=wl.omegas, T=t_chain, g_omegas=wl.omegas[::50], g=g_chain,
+                        dos=dos_chain, temps=temps, kappa=kappa_chain, omega_unit_rad_s=wl.omega_unit_rad_s,
+                        n_layers=8, eta=1e-8)
+
+    # ---- slab (n = 48): a stratified subsample of the 2048 x 64 grid -------
+    wl = W.slab_workload()
+    wsel = np.array([40, 300, 600, 900, 1200, 1500, 1800, 1950, 2047])
+    ksel = np.array([0, 13, 31, 50])
+    pairs, t_slab = [], []
+    lead_at = {}
+    for ki in ksel:
+        lead_at[ki] = LeadBlocks(d00=wl.lead_l["d00"][ki], d01=wl.lead_l["d01"][ki], d10=wl.lead_l["d10"][ki])
+    for wi in wsel:
+        for ki in ksel:
+            dv = Device1D(onsite_blocks=[wl.onsite[ki, 0]] * wl.n_layers,
+                          coupling_blocks=[wl.coupling[ki, 0]] * (wl.n_layers - 1))
+            t_slab.append(R.transmission(float(wl.omegas[wi]), dv, lead_at[ki], lead_at[ki], eta=wl.eta))
+            pairs.append((wi, ki))
+    g_pts = [(600, 13), (1800, 50)]
+    g_slab = np.stack([R.surface_gf(float(wl.omegas[wi]), lead_at[ki].d00, lead_at[ki].d01, lead_at[ki].d10,
+                                    eta=wl.eta) for wi, ki in g_pts])
+    g_slab_qep = np.stack([R.surface_gf(float(wl.omegas[wi]), lead_at[ki].d00, lead_at[ki].d01, lead_at[ki].d10,
+                                        eta=wl.eta, method="generalized_eigen") for wi, ki in g_pts])
+    dos_slab = np.array([R.lead_surface_dos(float(wl.omegas[wi]), lead_at[ki], eta=wl.eta) for wi, ki in pairs])
+    np.savez_compressed(OUT / "slab.npz", omegas=wl.omegas[wsel], wsel=wsel, ksel=ksel,
+                        kpoints=np.array([wl.kpoints[k] for k in ksel]), pairs=np.array(pairs), T=np.array(t_slab),
+                        d00=wl.lead_l["d00"][ksel], d01=wl.lead_l["d01"][ksel], d10=wl.lead_l["d10"][ksel],
+                        onsite=wl.onsite[ksel, 0], coupling=wl.coupling[ksel, 0], n_layers=wl.n_layers,
+                        eta=wl.eta, omega_max=wl.omega_max, g_pts=np.array(g_pts), g=g_slab, g_qep=g_slab_qep,
+                        dos=dos_slab)
+
+    # ---- negfpy test-suite systems ----------------------------------------
+    cases = {}
+    # matched chain plateau, L = 20 (tests/test_chain_transmission.py)
+    wmax = 2.0
+    om = np.linspace(0.2 * wmax, 0.8 * wmax, 9)
+    d20 = device_perfect_chain(20, p)
+    cases["chain_plateau_T"] = np.array([R.transmission(float(w), d20, lead, lead, eta=1e-8) for w in om])
+    cases["chain_plateau_omega"] = om
+    om = np.linspace(1.1 * wmax, 1.7 * wmax, 10)
+    d16 = device_perfect_chain(16, p)
+    cases["chain_outband_T"] = np.array([R.transmission(float(w), d16, lead, lead, eta=1e-8) for w in om])
+    cases["chain_outband_omega"] = om
+    # rectangular contact with a decoupled padding DOF (tests/test_interface_contacts.py)
+    lead1 = LeadBlocks(d00=np.array([[2.0]], dtype=np.complex128), d01=np.array([[-1.0]], dtype=np.complex128))
+    onsite = [np.diag([2.0, 100.0]).astype(np.complex128) for _ in range(4)]
+    coupling = [np.diag([-1.0, 0.0]).astype(np.complex128) for _ in range(3)]
+    cases["rect_T"] = np.array(R.transmission(1.0, Device1D(onsite, coupling), lead1, lead1, eta=1e-8,
+                                              device_to_lead_left=np.array([[-1.0]]),
+                                              device_to_lead_right=np.array([[-1.0]]),
+                                              contact_left_indices=[0], contact_right_indices=[6]))
+    # square lattice with k (tests/test_kspace_transport.py)
+    sq = SquareLatticeParams(mass=1.0, spring_x=1.0, spring_y=0.5)
+    sql, sqd = square_lattice_lead(sq), square_lattice_device(25, sq)
+    kp = [(-np.pi,), (-np.pi / 3.0,), (0.0,), (np.pi / 3.0,), (np.pi,)]
+    cases["square_kpoints"] = np.array(kp)
+    cases["square_T"] = np.array([R.transmission(0.9, sqd, sql, sql, kpar=k) for k in kp])
+    cases["square_kavg"] = np.array(R.transmission_kavg(0.9, sqd, sql, sql, kpoints=kp))
+    # multi-DOF channel plateau (tests/test_multidof_transport.py)
+    md = MultiDofCellParams(masses=np.ones(2), fc00=2.0 * np.eye(6), fc01=-np.eye(6), dof_per_atom=3)
+    cases["multidof_T"] = np.array(R.transmission(1.0, multidof_device(30, md), multidof_lead_blocks(md),
+                                                  multidof_lead_blocks(md), eta=1e-8))
+    # omega_scale and a separate device eta on the slab system
+    dv = Device1D(onsite_blocks=[wl.onsite[13, 0]] * 6, coupling_blocks=[wl.coupling[13, 0]] * 5)
+    cases["slab_scaled_T"] = np.array(R.transmission(float(wl.omegas[900]), dv, lead_at[13], lead_at[13],
+                                                     eta=wl.eta, eta_device=3.0 * wl.eta, omega_scale=1.7))
+    # adaptive ladder on the chain (tests/test_chain_transmission.py)
+    d14 = device_perfect_chain(14, p)
+    tav, info = R.transmission_kavg_adaptive(1.0, d14, lead, lead, kpoints=[(), (), ()], eta_values=(1e-8, 1e-7),
+                                             min_success_fraction=1.0)
+    cases["chain_adaptive_T"] = np.array(tav)
+    np.savez_compressed(OUT / "cases.npz", **cases)
+    print("wrote", sorted(p.name for p in OUT.glob("*.npz")))
+
+
+if __name__ == "__main__":
+    main()

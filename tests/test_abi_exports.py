@@ -1,0 +1,35 @@
+"""The C-ABI library builds, loads without a GPU and exports every declared symbol."""
+
+import re
+from pathlib import Path
+
+from negfpy_b200 import _build, _lib
+
+HEADER = Path(__file__).resolve().parents[1] / "include" / "negf_b200.h"
+
+
+def declared_symbols() -> set[str]:
+    text = HEADER.read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return set(re.findall(r"\b(negf_[a-z0-9_]+)\s*\(", text))
+
+
+def test_library_loads_and_exports_header_symbols():
+    lib = _lib.load()
+    decl = declared_symbols()
+    assert decl, "no declarations parsed"
+    for name in decl:
+        assert hasattr(lib, name), name
+    assert decl == set(_lib.exported_symbols())
+    assert lib.negf_get_version() == 1
+
+
+def test_workspace_query_without_gpu_is_safe():
+    lib = _lib.load()
+    # size queries for unsupported orders return 0 rather than touching a device
+    assert lib.negf_rgf_workspace_bytes(0, 1, 1) == 0
+    assert lib.negf_rgf_workspace_bytes(1, 1, 1) == 256
+
+
+def test_build_is_for_sm100a():
+    assert "arch=compute_100a,code=sm_100a" in " ".join(_build.ARCH)
