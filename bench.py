@@ -44,6 +44,10 @@ def _args():
     ap.add_argument("--cpu-sample", type=int, default=0, help="points in the CPU baseline sample (0 = auto)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--omegas", type=int, default=N_OMEGA,
+                    help="omegas per rank (default: the full 2048; smaller values are profiling cases)")
+    ap.add_argument("--kernels-only", action="store_true",
+                    help="time the kernels only (no e2e, CPU baseline or peak probe); for profiling runs")
     return ap.parse_args()
 
 
@@ -54,11 +58,17 @@ def _dist():
     return ws, rank, local
 
 
-def _workload(rank: int, world: int):
+def _workload(rank: int, world: int, n_omega: int = N_OMEGA):
+    """The slab grid of N_OMEGA*world omegas; this rank's omega indices.
+
+    ``n_omega`` < N_OMEGA keeps an evenly strided subset of the rank's shard
+    (a profiling case with the same frequency distribution)."""
     from negfpy_b200 import workloads as W
 
     wl = W.slab_workload(n_omega=N_OMEGA * world, n_k=N_K, n_layers=N_LAYERS)
     shard = np.arange(rank, N_OMEGA * world, world)
+    if n_omega < N_OMEGA:
+        shard = shard[:: max(1, N_OMEGA // n_omega)][:n_omega]
     return wl, shard
 
 
@@ -199,7 +209,7 @@ def main():
     from negfpy_b200 import engine, spectrum
 
     dev = torch.device("cuda", local)
-    wl, shard = _workload(rank, ws)
+    wl, shard = _workload(rank, ws, args.omegas)
     s = engine.StackedSystem.from_arrays(wl.lead_l, wl.lead_l, wl.onsite, wl.coupling, wl.n_layers)
     K = len(wl.kpoints)
     W = len(shard)
@@ -247,6 +257,15 @@ def main():
 
     status = st.cpu().numpy()
     iters = rl["iters"].cpu().numpy().astype(np.float64)
+    if args.kernels_only:
+        if rank == 0:
+            print(json.dumps({"kernels_only": True, "points_per_rank": P, "steps": args.steps,
+                              "s_sgf_per_step": t_sr / args.steps, "s_rgf_per_step": t_rgf / args.steps,
+                              "points_per_s": value, "mean_sgf_iterations": float(iters.mean()),
+                              "status_ok_fraction": float(np.mean(status == 0))}), flush=True)
+        if ws > 1:
+            dist.destroy_process_group()
+        return
     n = wl.n
     L = wl.n_layers
     # Algorithmic complex flops (8 real flops per complex multiply-add):

@@ -56,7 +56,7 @@ int negf_sgf_sr_f64(int n, int batch, const double* h00, const double* h01, cons
   a.status_out = status_out;
   int rc = negf::sr_f64_launch(a, as_stream(stream));
   if (rc == -2) return fail(NEGF_EUNSUPPORTED, "negf_sgf_sr_f64: block order not built");
-  if (rc != 0) return cuda_fail("negf_sgf_sr_f64");
+  if (rc != 0) return fail(NEGF_ECUDA, negf::last_launch_error());
   return 0;
 }
 
@@ -132,7 +132,7 @@ int negf_rgf_transmission_f64(int n_dev, int n_lead_l, int n_lead_r, int n_layer
     return cuda_fail("negf_rgf_transmission_f64: counter reset");
   int rc = negf::rgf_f64_launch(a, np, grid, st);
   if (rc == -2) return fail(NEGF_EUNSUPPORTED, "negf_rgf_transmission_f64: block order not built");
-  if (rc != 0) return cuda_fail("negf_rgf_transmission_f64");
+  if (rc != 0) return fail(NEGF_ECUDA, negf::last_launch_error());
   return 0;
 }
 

@@ -1,12 +1,18 @@
 // FP64 kernels of the per-(omega, k) phonon NEGF path.
 //
 // One thread block owns one (omega, k) point at a time.  Blocks of order
-// n <= 48 live entirely in shared memory, padded to NP (a multiple of the
-// thread-grid side TG) with a row stride of NP + 1 complex numbers so that
-// row and column walks are both bank-conflict free.  Thread (tr, tc) of the
-// TG x TG grid owns the RT x RT elements (tr + TG*i, tc + TG*j), RT = NP/TG,
-// in every matrix operation (products, Gauss-Jordan updates, epilogues), so
-// register-resident matrices line up with shared-memory ones.
+// n <= 48 live entirely in shared memory, zero-padded to NP in {16, 32, 48}.
+// Complex products run on the FP64 tensor path: mma.sync m16n8k8 f64, four
+// real MMAs per complex tile (re += ar br - ai bi, im += ar bi + ai br).
+// Warp w owns the 16 x 16 output region (16*(w / T), 16*(w % T)), T = NP/16,
+// as two 16 x 8 MMA tiles; in every elementwise phase (Gauss-Jordan updates,
+// epilogues, register-resident matrices) a thread owns exactly the eight
+// elements its MMA accumulators hold, so no data moves between phases.
+//
+// Shared matrices are stored as interleaved (re, im) pairs, row-major with
+// row stride NP, and the column index XOR-swizzled per row (see sidx) so the
+// A-fragment pattern (2 rows x 4 columns per 8 lanes) and the B-fragment /
+// conjugate-transpose pattern (4 rows x 2 columns) are both conflict-free.
 //
 //   sr_f64_kernel   Sancho-Rubio decimation (negfpy core/surface_gf.py:18-81):
 //                   alpha, beta, g = (z - eps)^-1, alpha g, beta g in shared
@@ -19,6 +25,8 @@
 //                   (:115-116) and T = Re Tr[Gamma_L G Gamma_R G^H] (:356).
 //   *_scalar_kernel the same for 1 x 1 blocks (the monatomic chain), one
 //                   thread per point.
+#include <cstdio>
+
 #include "negf_common.cuh"
 #include "negf_f64.h"
 
@@ -30,243 +38,509 @@ __device__ __forceinline__ double2 z_of(double w, double e) {
   return make_double2(__dsub_rn(__dmul_rn(w, w), __dmul_rn(e, e)), __dmul_rn(2.0 * w, e));
 }
 
-template <int NP, int TG>
+template <int NP>
 struct Geo {
-  static constexpr int RT = NP / TG;
-  static constexpr int LD = NP + 1;
-  static constexpr int MAT = NP * LD;  // complex elements per matrix buffer
-  static constexpr int NTH = TG * TG;
+  static constexpr int T = NP / 16;     // 16-row tiles per side
+  static constexpr int NW = T * T;      // warps, one 16 x 16 region each
+  static constexpr int NTH = 32 * NW;   // threads
+  static constexpr int MAT = NP * NP;   // complex elements per matrix buffer
 };
 
-// ---------------------------------------------------------------- products --
-// c = op(A) op(B) summed over k < kn; op = conjugate transpose when AC / BC.
-template <int NP, int TG, bool AC, bool BC>
-__device__ __forceinline__ void mm(double2 (&c)[NP / TG][NP / TG], const double2* __restrict__ A,
-                                   const double2* __restrict__ B, int kn, int tr, int tc) {
-  constexpr int RT = NP / TG, LD = NP + 1;
+// Row-dependent XOR swizzle of the column index (bits 0-2), values
+// {0, 5, 2, 7, 1, 4, 3, 6} for r mod 8 = 0..7.  With 16-byte elements and
+// phases of 8 lanes it makes every access pattern used here conflict-free:
+// A fragments (rows r, r+1 x 4 columns: bit 2 differs), B fragments and
+// conjugate-transpose walks (4 rows x 2 columns: bits 2-1 distinct),
+// accumulator stores (rows r, r+1 x even columns: bit 0 differs) and column
+// walks (8 rows: all distinct).
+__device__ __forceinline__ int swz(int r) { return (int)((0xCE1EA8u >> (3 * (r & 7))) & 7u); }
+template <int NP>
+__device__ __forceinline__ int sidx(int r, int c) { return r * NP + (c ^ swz(r)); }
+
+// Lane geometry of the warp's 16 x 16 region.
+struct Lane {
+  int g, t, m0, n0;
+};
+template <int NP>
+__device__ __forceinline__ Lane lane_geo() {
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  Lane L;
+  L.g = l >> 2;
+  L.t = l & 3;
+  L.m0 = (w / Geo<NP>::T) * 16;
+  L.n0 = (w % Geo<NP>::T) * 16;
+  return L;
+}
+// Element (row, col) held in accumulator slot q of tile j (8 slots per thread).
+__device__ __forceinline__ int own_r(const Lane& L, int q) { return L.m0 + L.g + 8 * (q >> 1); }
+__device__ __forceinline__ int own_c(const Lane& L, int j, int q) { return L.n0 + 8 * j + 2 * L.t + (q & 1); }
+
+// Complex accumulators of the warp's two 16 x 8 tiles.
+struct CAcc {
+  double re[2][4], im[2][4];
+  __device__ __forceinline__ void zero() {
 #pragma unroll
-  for (int i = 0; i < RT; ++i)
+    for (int j = 0; j < 2; ++j)
 #pragma unroll
-    for (int j = 0; j < RT; ++j) c[i][j] = make_double2(0.0, 0.0);
-#pragma unroll 2
-  for (int k = 0; k < kn; ++k) {
-    double2 a[RT], b[RT];
+      for (int q = 0; q < 4; ++q) re[j][q] = im[j][q] = 0.0;
+  }
+  __device__ __forceinline__ double2 get(int j, int q) const { return make_double2(re[j][q], im[j][q]); }
+};
+
+__device__ __forceinline__ void dmma(double (&d)[4], const double (&a)[4], double b0, double b1) {
+  asm("mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
+      : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+      : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b0), "d"(b1));
+}
+
+// Fragment addressing.  Chunk k0 (a multiple of 8) never changes an index
+// modulo 8, so every fragment address is a loop-invariant base plus k0
+// (row-major walk) or k0 * NP (column walk).
+//   A = S     : (m0+g+8(q&1), k0+t+4(q>>1)) -> base + k0
+//   A = S^H   : S(k0+t+4(q>>1), m0+g+8(q&1)) -> base + k0*NP
+//   B = S     : S(k0+t+4q, nb+g)             -> base + k0*NP
+//   B = S^H   : S(nb+g, k0+t+4q)             -> base + k0
+template <int NP, bool CT>
+__device__ __forceinline__ void a_bases(const Lane& L, int (&base)[4]) {
 #pragma unroll
-    for (int i = 0; i < RT; ++i) a[i] = AC ? cconj(A[k * LD + tr + TG * i]) : A[(tr + TG * i) * LD + k];
+  for (int q = 0; q < 4; ++q) {
+    const int r = L.m0 + L.g + 8 * (q & 1), kk = L.t + 4 * (q >> 1);
+    base[q] = CT ? sidx<NP>(kk, r) : sidx<NP>(r, kk);
+  }
+}
+// A fragment bases into a row-stride-8 panel (16 x 8 at rows m0..).
+__device__ __forceinline__ void a_bases8(const Lane& L, int (&base)[4]) {
 #pragma unroll
-    for (int j = 0; j < RT; ++j) b[j] = BC ? cconj(B[(tc + TG * j) * LD + k]) : B[k * LD + tc + TG * j];
+  for (int q = 0; q < 4; ++q) {
+    const int r = L.m0 + L.g + 8 * (q & 1), kk = L.t + 4 * (q >> 1);
+    base[q] = r * 8 + (kk ^ swz(r));
+  }
+}
+template <int NP, bool CT>
+__device__ __forceinline__ void b_bases(const Lane& L, int (&base)[2][2]) {
 #pragma unroll
-    for (int i = 0; i < RT; ++i)
+  for (int j = 0; j < 2; ++j)
 #pragma unroll
-      for (int j = 0; j < RT; ++j) cfma(c[i][j], a[i], b[j]);
+    for (int q = 0; q < 2; ++q) {
+      const int kk = L.t + 4 * q, c = L.n0 + 8 * j + L.g;
+      base[j][q] = CT ? sidx<NP>(c, kk) : sidx<NP>(kk, c);
+    }
+}
+template <int NP, bool CT>
+__device__ __forceinline__ void load_a(const double2* __restrict__ S, const int (&base)[4], int k0, double (&ar)[4],
+                                       double (&ai)[4]) {
+  const int off = CT ? k0 * NP : k0;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const double2 v = S[base[q] + off];
+    ar[q] = v.x;
+    ai[q] = CT ? -v.y : v.y;
+  }
+}
+template <int NP, bool CT>
+__device__ __forceinline__ void load_b(const double2* __restrict__ S, const int (&base)[2], int k0, double (&br)[2],
+                                       double (&bi)[2]) {
+  const int off = CT ? k0 : k0 * NP;
+#pragma unroll
+  for (int q = 0; q < 2; ++q) {
+    const double2 v = S[base[q] + off];
+    br[q] = v.x;
+    bi[q] = CT ? -v.y : v.y;
+  }
+}
+__device__ __forceinline__ void cmma(double (&cr)[4], double (&ci)[4], const double (&ar)[4], const double (&ai)[4],
+                                     const double (&br)[2], const double (&bi)[2]) {
+  dmma(cr, ar, br[0], br[1]);
+  dmma(cr, ai, -bi[0], -bi[1]);
+  dmma(ci, ar, bi[0], bi[1]);
+  dmma(ci, ai, br[0], br[1]);
+}
+
+// c = op(A) op(B) over the first kch chunks of 8 (the rest is zero padding).
+template <int NP, bool AC, bool BC>
+__device__ __forceinline__ void cmm(CAcc& c, const double2* A, const double2* B, int kch, const Lane& L) {
+  int ab[4], bb[2][2];
+  a_bases<NP, AC>(L, ab);
+  b_bases<NP, BC>(L, bb);
+  c.zero();
+  for (int kc = 0; kc < kch; ++kc) {
+    double ar[4], ai[4];
+    load_a<NP, AC>(A, ab, kc * 8, ar, ai);
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      double br[2], bi[2];
+      load_b<NP, BC>(B, bb[j], kc * 8, br, bi);
+      cmma(c.re[j], c.im[j], ar, ai, br, bi);
+    }
+  }
+}
+// c1 = A1 B, c2 = A2 B.
+template <int NP>
+__device__ __forceinline__ void cmm2b(CAcc& c1, CAcc& c2, const double2* A1, const double2* A2, const double2* B,
+                                      int kch, const Lane& L) {
+  int ab[4], bb[2][2];
+  a_bases<NP, false>(L, ab);
+  b_bases<NP, false>(L, bb);
+  c1.zero();
+  c2.zero();
+  for (int kc = 0; kc < kch; ++kc) {
+    double a1r[4], a1i[4], a2r[4], a2i[4];
+    load_a<NP, false>(A1, ab, kc * 8, a1r, a1i);
+    load_a<NP, false>(A2, ab, kc * 8, a2r, a2i);
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      double br[2], bi[2];
+      load_b<NP, false>(B, bb[j], kc * 8, br, bi);
+      cmma(c1.re[j], c1.im[j], a1r, a1i, br, bi);
+      cmma(c2.re[j], c2.im[j], a2r, a2i, br, bi);
+    }
   }
 }
 
-// c1 = A1 B, c2 = A2 B: two products sharing the right operand.
-template <int NP, int TG>
-__device__ __forceinline__ void mm2b(double2 (&c1)[NP / TG][NP / TG], double2 (&c2)[NP / TG][NP / TG],
-                                     const double2* __restrict__ A1, const double2* __restrict__ A2,
-                                     const double2* __restrict__ B, int kn, int tr, int tc) {
-  constexpr int RT = NP / TG, LD = NP + 1;
+template <int NP>
+__device__ __forceinline__ void store_acc(double2* S, const CAcc& c, const Lane& L) {
 #pragma unroll
-  for (int i = 0; i < RT; ++i)
+  for (int j = 0; j < 2; ++j)
 #pragma unroll
-    for (int j = 0; j < RT; ++j) c1[i][j] = c2[i][j] = make_double2(0.0, 0.0);
-#pragma unroll 2
-  for (int k = 0; k < kn; ++k) {
-    double2 a1[RT], a2[RT], b[RT];
-#pragma unroll
-    for (int j = 0; j < RT; ++j) b[j] = B[k * LD + tc + TG * j];
-#pragma unroll
-    for (int i = 0; i < RT; ++i) {
-      a1[i] = A1[(tr + TG * i) * LD + k];
-      a2[i] = A2[(tr + TG * i) * LD + k];
-    }
-#pragma unroll
-    for (int i = 0; i < RT; ++i)
-#pragma unroll
-      for (int j = 0; j < RT; ++j) {
-        cfma(c1[i][j], a1[i], b[j]);
-        cfma(c2[i][j], a2[i], b[j]);
-      }
-  }
+    for (int q = 0; q < 4; ++q) S[sidx<NP>(own_r(L, q), own_c(L, j, q))] = c.get(j, q);
 }
 
-// c1 = A1 B1, c2 = A2 B2.
-template <int NP, int TG>
-__device__ __forceinline__ void mmpair(double2 (&c1)[NP / TG][NP / TG], double2 (&c2)[NP / TG][NP / TG],
-                                       const double2* __restrict__ A1, const double2* __restrict__ B1,
-                                       const double2* __restrict__ A2, const double2* __restrict__ B2, int kn,
-                                       int tr, int tc) {
-  constexpr int RT = NP / TG, LD = NP + 1;
-#pragma unroll
-  for (int i = 0; i < RT; ++i)
-#pragma unroll
-    for (int j = 0; j < RT; ++j) c1[i][j] = c2[i][j] = make_double2(0.0, 0.0);
-#pragma unroll 2
-  for (int k = 0; k < kn; ++k) {
-    double2 a1[RT], a2[RT], b1[RT], b2[RT];
-#pragma unroll
-    for (int j = 0; j < RT; ++j) {
-      b1[j] = B1[k * LD + tc + TG * j];
-      b2[j] = B2[k * LD + tc + TG * j];
-    }
-#pragma unroll
-    for (int i = 0; i < RT; ++i) {
-      a1[i] = A1[(tr + TG * i) * LD + k];
-      a2[i] = A2[(tr + TG * i) * LD + k];
-    }
-#pragma unroll
-    for (int i = 0; i < RT; ++i)
-#pragma unroll
-      for (int j = 0; j < RT; ++j) {
-        cfma(c1[i][j], a1[i], b1[j]);
-        cfma(c2[i][j], a2[i], b2[j]);
-      }
-  }
-}
-
-template <int NP, int TG>
-__device__ __forceinline__ void store_tile(double2* S, const double2 (&c)[NP / TG][NP / TG], int tr, int tc) {
-  constexpr int RT = NP / TG, LD = NP + 1;
-#pragma unroll
-  for (int i = 0; i < RT; ++i)
-#pragma unroll
-    for (int j = 0; j < RT; ++j) S[(tr + TG * i) * LD + tc + TG * j] = c[i][j];
-}
-
-// Global n_r x n_c row-major matrix -> padded shared buffer (zeros outside).
-template <int NP, int TG>
+// Global nr x nc row-major matrix -> padded shared buffer (zeros outside).
+template <int NP>
 __device__ __forceinline__ void load_mat(double2* S, const double2* __restrict__ G, int nr, int nc) {
-  constexpr int LD = NP + 1, NTH = TG * TG;
-  for (int idx = threadIdx.x; idx < NP * NP; idx += NTH) {
-    int r = idx / NP, c = idx - r * NP;
-    S[r * LD + c] = (r < nr && c < nc) ? G[(long long)r * nc + c] : make_double2(0.0, 0.0);
+  for (int idx = threadIdx.x; idx < NP * NP; idx += Geo<NP>::NTH) {
+    const int r = idx / NP, c = idx - r * NP;
+    S[sidx<NP>(r, c)] = (r < nr && c < nc) ? G[(long long)r * nc + c] : make_double2(0.0, 0.0);
   }
+}
+
+// 1 / (a + ib) by Smith's algorithm (R. L. Smith, CACM 5(8), 1962).
+__device__ __forceinline__ double2 crecip_smith(double2 v) {
+  if (fabs(v.x) >= fabs(v.y)) {
+    const double r = v.y / v.x;
+    const double i = 1.0 / fma(v.y, r, v.x);
+    return make_double2(i, -r * i);
+  }
+  const double r = v.x / v.y;
+  const double i = 1.0 / fma(v.x, r, v.y);
+  return make_double2(r * i, -i);
+}
+
+// 2^(1023 - e) for the larger component exponent e of v: scales v so that
+// max(|re|, |im|) lies in [1, 2).  1 for zero/subnormal or huge components.
+__device__ __forceinline__ double pow2_normalizer(double2 v) {
+  const int ha = __double2hiint(v.x) & 0x7fffffff, hb = __double2hiint(v.y) & 0x7fffffff;
+  const int e = (ha > hb ? ha : hb) >> 20;
+  return (e != 0 && e < 2046) ? __hiloint2double((2046 - e) << 20, 0) : 1.0;
+}
+
+// 1 / p for a nonzero, finite complex p without FP64 division: p is scaled
+// by a power of two sc (exact) so that max(|re|, |im|) of p sc lies in
+// [1, 2); 1/|p sc|^2 comes from an fp32 reciprocal seed refined by two
+// Newton-Raphson steps y <- y + y (1 - d y) in FP64 (quadratic convergence:
+// 2^-22 -> 2^-44 -> below FP64 rounding); 1/p = sc conj(p sc) y.  Values
+// whose larger component is subnormal or near overflow use Smith's
+// algorithm instead.
+__device__ __forceinline__ float rcp_approx_f32(float x) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ double2 crecip_fast(double2 v) {
+  const int ha = __double2hiint(v.x) & 0x7fffffff, hb = __double2hiint(v.y) & 0x7fffffff;
+  const int e = (ha > hb ? ha : hb) >> 20;
+  if (e == 0 || e >= 2046) return crecip_smith(v);
+  const double sc = __hiloint2double((2046 - e) << 20, 0);  // 2^(1023 - e)
+  const double as = v.x * sc, bs = v.y * sc;
+  const double d = fma(as, as, bs * bs);  // in [1, 8)
+  double y = (double)rcp_approx_f32((float)d);
+  y = fma(y, fma(-d, y, 1.0), y);
+  y = fma(y, fma(-d, y, 1.0), y);
+  return make_double2((as * y) * sc, -(bs * y) * sc);
 }
 
 // ---------------------------------------------------------- Gauss-Jordan --
-// In-place inverse of the leading n x n block of M (the padding must hold the
-// identity) by Gauss-Jordan elimination with partial pivoting on |re| + |im|
-// (the pivot measure of LAPACK's getrf).  Row interchanges are undone as
-// column interchanges at the end.  Returns kOk, kSingular (exact zero pivot)
-// or kNonFinite, identically in every thread.
-struct GJScratch {
-  double2* rowk;   // scaled pivot row
-  double2* colk;   // pivot column after the interchange
-  double2* oldrk;  // pivot row before the interchange
-  int* perm;       // interchange record
-  int* piv;        // [0] pivot row, [1] status
+// Shared bookkeeping of the blocked Gauss-Jordan inversion (the panel itself
+// lives in a caller-provided free matrix buffer).
+struct GJShared {
+  int* sig;       // logical -> physical row within the current panel
+  int* siginv;    // physical -> logical
+  int* pivlog;    // pivlog[k]: logical row interchanged with row k at step k
+  unsigned* key;  // [8] pivot key of each panel column
 };
+template <int NP>
+__host__ __device__ constexpr int gj_shared_bytes() { return 3 * NP * 4 + 8 * 4; }
+template <int NP>
+__device__ __forceinline__ GJShared carve_gj(unsigned char* base) {
+  GJShared g;
+  g.sig = reinterpret_cast<int*>(base);
+  g.siginv = g.sig + NP;
+  g.pivlog = g.siginv + NP;
+  g.key = reinterpret_cast<unsigned*>(g.pivlog + NP);
+  return g;
+}
+// Panel element (row r, column c < 8), rows of 8 with the row swizzle.
+__device__ __forceinline__ int pidx(int r, int c) { return r * 8 + (c ^ swz(r)); }
 
-template <int NP, int TG>
-__device__ int gj_invert(double2* M, int n, const GJScratch& s) {
-  constexpr int RT = NP / TG, LD = NP + 1, NTH = TG * TG;
-  const int tid = threadIdx.x, tr = tid / TG, tc = tid - tr * TG;
-  for (int k = 0; k < n; ++k) {
-    if (tid < 32) {
-      double best = -1.0;
-      int bi = n;
-      for (int i = k + tid; i < n; i += 32) {
-        double v = cabs1(M[i * LD + k]);
-        if (v > best) { best = v; bi = i; }
-      }
+// Pivot key of a candidate entry: top bits of max(|re|, |im|) with the row
+// index (< 64) in the low 6 bits, so the unsigned maximum over a column picks
+// the largest entry up to a relative 2^-14, ties to the lowest row.
+__device__ __forceinline__ unsigned pivot_key(double2 v, int r) {
+  const unsigned ha = (unsigned)__double2hiint(v.x) & 0x7fffffffu;
+  const unsigned hb = (unsigned)__double2hiint(v.y) & 0x7fffffffu;
+  const unsigned hm = ha > hb ? ha : hb;
+  return (hm & ~63u) | (unsigned)(63 - r);
+}
+
+// Inverse of the leading n x n block of X (padding = identity, n <= NP <= 64)
+// by blocked Gauss-Jordan elimination with partial pivoting.  Y is the second
+// matrix buffer and Z (at least 2 NP x 8 complex) holds the panel; *out
+// receives the buffer holding the inverse (X or Y).
+//
+// Columns are processed in panels of 8.  The n x 8 panel is factored by the
+// whole block with one barrier per column and no division: the panel is kept
+// as W = lambda P (P the textbook Gauss-Jordan panel, lambda a complex
+// scalar) and, with p the pivot and s a power of two bringing p near 1,
+//     new(r, c) = (p s) a' - (s b') m,   lambda <- lambda p s
+//     a' = 0 if r is the pivot row or c the pivot column, else W(r, c)
+//     b' = -lambda for the pivot row, else W(r, j)
+//     m  =  lambda for the pivot column, else W(pivot row, c)
+// (expanding W = lambda P gives the textbook update times the new lambda;
+// |p s| lies in [1, 2.83]).  Pivot search is looked ahead: the threads that
+// write column j+1 of the panel reduce its pivot keys (see pivot_key) over
+// the rows not yet used as pivots into key[j+1] before the barrier, so step
+// j+1 starts from one shared load; the key's exponent bits give s.  The row
+// interchanges are kept as a permutation (sig).  Then every warp applies the
+// panel to the whole matrix as a rank-8 product on the FP64 tensor path,
+// writing the next buffer in the new row order:
+//     next(r, Q) = [r not a pivot row] W(sig r, Q) + P(sig r, :) W(sig(pivot rows), Q)
+//     next(r, panel) = P(sig r, :),   P = W / lambda
+// The interchanges are undone at the end as column interchanges (column c of
+// the inverse is column t_{n-1}(...t_0(c)) of the eliminated matrix,
+// t_k = (k pivlog_k)) in one gather.  Returns kOk, kSingular (all candidates
+// zero or below 2^-1022) or kNonFinite identically in every thread.
+template <int NP>
+__device__ int gj_invert(double2* X, double2* Y, double2* Z, int n, const Lane& L, const GJShared& sh,
+                         double2** out) {
+  static_assert(NP <= 64, "pivot keys carry a 6-bit row index");
+  constexpr int NTH = Geo<NP>::NTH;
+  constexpr int PE = NP * 8;                  // panel elements
+  constexpr int PPT = (PE + NTH - 1) / NTH;   // panel elements per thread
+  const int tid = threadIdx.x, lane = tid & 31;
+  double2* cur = X;
+  double2* nxt = Y;
+  int rows[2], rbase[2], rsw[2];
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        double ov = __shfl_xor_sync(0xffffffffu, best, o);
-        int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-        if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
-      }
-      if (tid == 0) {
-        s.piv[0] = bi;
-        s.piv[1] = (best > 0.0) ? (int)kOk : (best == 0.0 ? (int)kSingular : (int)kNonFinite);
-      }
-    }
-    __syncthreads();
-    const int pr = s.piv[0];
-    const int bad = s.piv[1];
-    if (bad) return bad;
-    const double2 piv = M[pr * LD + k];
-    const double2 ip = crecip(piv);
-    for (int t = tid; t < n; t += NTH) {
-      double2 rk = M[k * LD + t];
-      s.oldrk[t] = rk;
-      s.rowk[t] = (t == k) ? ip : cmul(M[pr * LD + t], ip);
-      s.colk[t] = (t == k) ? piv : ((t == pr) ? M[k * LD + k] : M[t * LD + k]);
-    }
-    if (tid == 0) s.perm[k] = pr;
-    __syncthreads();
-#pragma unroll
-    for (int i = 0; i < RT; ++i) {
-      const int r = tr + TG * i;
-      if (r >= n) continue;
-      const double2 ci = s.colk[r];
-#pragma unroll
-      for (int j = 0; j < RT; ++j) {
-        const int c = tc + TG * j;
-        if (c >= n) continue;
-        double2 v;
-        if (r == k) {
-          v = s.rowk[c];
-        } else if (c == k) {
-          v = cneg(cmul(ci, ip));
-        } else {
-          v = (r == pr) ? s.oldrk[c] : M[r * LD + c];
-          cfma(v, cneg(ci), s.rowk[c]);
-        }
-        M[r * LD + c] = v;
-      }
-    }
-    __syncthreads();
+  for (int ri = 0; ri < 2; ++ri) {
+    rows[ri] = L.m0 + L.g + 8 * ri;
+    rbase[ri] = rows[ri] * NP;
+    rsw[ri] = swz(rows[ri]);
   }
-  for (int r = tid; r < n; r += NTH) {
-    for (int k = n - 1; k >= 0; --k) {
-      const int q = s.perm[k];
-      if (q != k) {
-        double2 t = M[r * LD + k];
-        M[r * LD + k] = M[r * LD + q];
-        M[r * LD + q] = t;
+  int cols[4], scol[4];
+#pragma unroll
+  for (int ci = 0; ci < 4; ++ci) cols[ci] = scol[ci] = L.n0 + 8 * (ci >> 1) + 2 * L.t + (ci & 1);
+  // panel elements owned by this thread
+  int pr_[PPT], pc_[PPT];
+  bool pin[PPT];
+#pragma unroll
+  for (int q = 0; q < PPT; ++q) {
+    const int e = tid + q * NTH;
+    pin[q] = e < PE;
+    pr_[q] = pin[q] ? (e >> 3) : 0;
+    pc_[q] = e & 7;
+  }
+
+  for (int k0 = 0; k0 < n; k0 += 8) {
+    const int jmax = (n - k0) < 8 ? (n - k0) : 8;
+    double2* P = Z;
+    double2* Pn = Z + PE;
+    bool used[PPT];
+    // ---- load the panel, reset the bookkeeping, keys of panel column 0 ----
+    unsigned key0 = 0u;
+#pragma unroll
+    for (int q = 0; q < PPT; ++q) {
+      const int r = pr_[q], c = pc_[q];
+      used[q] = false;
+      if (pin[q]) {
+        const double2 v = cur[sidx<NP>(r, k0 + c)];
+        P[pidx(r, c)] = v;
+        if (c == 0 && r >= k0 && r < n) key0 = max(key0, pivot_key(v, r));
       }
     }
+    for (int r = tid; r < NP; r += NTH) {
+      sh.sig[r] = r;
+      sh.siginv[r] = r;
+    }
+    if (tid < 8) sh.key[tid] = 0u;
+    __syncthreads();
+    key0 = __reduce_max_sync(0xffffffffu, key0);
+    if (lane == 0 && key0) atomicMax(&sh.key[0], key0);
+    __syncthreads();
+    double2 lam = make_double2(1.0, 0.0);
+    // ---- factor the panel, one barrier per column ----
+    for (int j = 0; j < jmax; ++j) {
+      const unsigned key = sh.key[j];
+      if ((key >> 20) >= 0x7ffu) return kNonFinite;
+      if ((key >> 6) == 0u) return kSingular;
+      const int pr = 63 - (int)(key & 63u);
+      const int ex = (int)(key >> 20);
+      const double sc = (ex != 0 && ex < 2046) ? __hiloint2double((2046 - ex) << 20, 0) : 1.0;
+      if (tid == 0) {
+        const int k = k0 + j;
+        const int bl = sh.siginv[pr];
+        const int pa = sh.sig[k];
+        sh.sig[k] = pr;
+        sh.sig[bl] = pa;
+        sh.siginv[pr] = k;
+        sh.siginv[pa] = bl;
+        sh.pivlog[k] = bl;
+      }
+      const double2 piv = P[pidx(pr, j)];
+      double2 mv[PPT], fv[PPT], av[PPT];
+#pragma unroll
+      for (int q = 0; q < PPT; ++q) {
+        mv[q] = P[pidx(pr, pc_[q])];
+        fv[q] = P[pidx(pr_[q], j)];
+        av[q] = P[pidx(pr_[q], pc_[q])];
+      }
+      const double2 ps = make_double2(piv.x * sc, piv.y * sc);
+      unsigned nk = 0u;
+#pragma unroll
+      for (int q = 0; q < PPT; ++q) {
+        const int r = pr_[q], c = pc_[q];
+        const bool isp = (r == pr);
+        used[q] = used[q] || isp;
+        const double2 bb = isp ? cneg(lam) : fv[q];
+        const double2 b = make_double2(bb.x * sc, bb.y * sc);
+        const double2 m = (c == j) ? lam : mv[q];
+        double2 v = cneg(cmul(b, m));
+        if (!isp && c != j) cfma(v, ps, av[q]);
+        if (pin[q]) {
+          Pn[pidx(r, c)] = v;
+          if (c == j + 1 && !used[q] && r >= k0 && r < n) nk = max(nk, pivot_key(v, r));
+        }
+      }
+      lam = cmul(lam, ps);
+      if (j + 1 < jmax) {
+        nk = __reduce_max_sync(0xffffffffu, nk);
+        if (lane == 0 && nk) atomicMax(&sh.key[j + 1], nk);
+      }
+      __syncthreads();
+      double2* t = P;
+      P = Pn;
+      Pn = t;
+    }
+    // ---- rank-8 update of the whole matrix (all warps) ----
+    const double2 il = crecip_smith(lam);
+    CAcc c;
+    int srow[2];
+    bool inpanel[2];
+#pragma unroll
+    for (int ri = 0; ri < 2; ++ri) {
+      srow[ri] = sh.sig[rows[ri]];
+      inpanel[ri] = rows[ri] >= k0 && rows[ri] < k0 + jmax;
+    }
+#pragma unroll
+    for (int j2 = 0; j2 < 2; ++j2)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int ri = q >> 1, cc = own_c(L, j2, q);
+        const double2 v = cur[sidx<NP>(srow[ri], cc)];
+        c.re[j2][q] = inpanel[ri] ? 0.0 : v.x;
+        c.im[j2][q] = inpanel[ri] ? 0.0 : v.y;
+      }
+    {
+      double ar[4], ai[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int kk = L.t + 4 * (q >> 1);
+        const double2 v = cmul(P[pidx(srow[q & 1], kk)], il);
+        ar[q] = v.x;
+        ai[q] = v.y;
+      }
+      const int kk0 = L.t, kk1 = L.t + 4;
+      const int pr0 = kk0 < jmax ? sh.sig[k0 + kk0] : 0, pr1 = kk1 < jmax ? sh.sig[k0 + kk1] : 0;
+#pragma unroll
+      for (int j2 = 0; j2 < 2; ++j2) {
+        const int cc = L.n0 + 8 * j2 + L.g;
+        const double2 v0 = cur[sidx<NP>(pr0, cc)], v1 = cur[sidx<NP>(pr1, cc)];
+        double br[2], bi[2];
+        br[0] = kk0 < jmax ? v0.x : 0.0;
+        bi[0] = kk0 < jmax ? v0.y : 0.0;
+        br[1] = kk1 < jmax ? v1.x : 0.0;
+        bi[1] = kk1 < jmax ? v1.y : 0.0;
+        cmma(c.re[j2], c.im[j2], ar, ai, br, bi);
+      }
+    }
+#pragma unroll
+    for (int j2 = 0; j2 < 2; ++j2)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int r = own_r(L, q), cc = own_c(L, j2, q);
+        double2 v = c.get(j2, q);
+        if (cc >= k0 && cc < k0 + 8) v = cmul(P[pidx(srow[q >> 1], cc - k0)], il);
+        nxt[sidx<NP>(r, cc)] = v;
+      }
+    for (int j = 0; j < jmax; ++j) {
+      const int k = k0 + j, b2 = sh.pivlog[k];
+#pragma unroll
+      for (int ci = 0; ci < 4; ++ci) {
+        const int scc = scol[ci];
+        scol[ci] = (scc == k) ? b2 : ((scc == b2) ? k : scc);
+      }
+    }
+    __syncthreads();
+    double2* t = cur;
+    cur = nxt;
+    nxt = t;
+  }
+#pragma unroll
+  for (int e = 0; e < 8; ++e) {
+    const int ri = (e & 3) >> 1, ci = (e >> 2) * 2 + (e & 1);
+    nxt[rbase[ri] + (cols[ci] ^ rsw[ri])] = cur[rbase[ri] + (scol[ci] ^ rsw[ri])];
   }
   __syncthreads();
+  *out = nxt;
   return kOk;
 }
 
-template <int NP, int TG>
-__device__ __forceinline__ GJScratch carve_gj(double2* base) {
-  GJScratch s;
-  s.rowk = base;
-  s.colk = base + NP;
-  s.oldrk = base + 2 * NP;
-  s.perm = reinterpret_cast<int*>(base + 3 * NP);
-  s.piv = s.perm + NP;
-  return s;
-}
-// Bytes after the matrix buffers: GJ vectors, perm/pivot ints, reduction slots.
+// Bytes after the matrix buffers: Gauss-Jordan scratch, then reduction slots.
 template <int NP>
-constexpr int tail_bytes() { return 3 * NP * 16 + ((NP + 4) * 4 + 15) / 16 * 16 + 40 * 8; }
+__host__ __device__ constexpr int tail_bytes() { return gj_shared_bytes<NP>() + 40 * 8; }
+template <int NP>
+__device__ __forceinline__ double* carve_red(double2* tail) {
+  return reinterpret_cast<double*>(reinterpret_cast<unsigned char*>(tail) + gj_shared_bytes<NP>());
+}
 
 // ------------------------------------------------------------ Sancho-Rubio --
-template <int NP, int TG>
-__global__ void __launch_bounds__(TG* TG, 1) sr_f64_kernel(SrArgs a) {
-  using G = Geo<NP, TG>;
-  constexpr int RT = G::RT, LD = G::LD, MAT = G::MAT;
+// Shared buffers: alpha, beta, g (inverse, then the next alpha), alpha g,
+// beta g, eps_s.  eps lives in registers.  Every thread reads and writes
+// only its own elements of eps and eps_s, so those need no barriers.
+template <int NP>
+constexpr int sr_buffers() { return 6; }
+
+template <int NP>
+__global__ void __launch_bounds__(Geo<NP>::NTH, 1) sr_f64_kernel(SrArgs a) {
+  using G = Geo<NP>;
+  constexpr int MAT = G::MAT;
   extern __shared__ __align__(16) unsigned char smraw[];
-  double2* sA = reinterpret_cast<double2*>(smraw);
-  double2* sB = sA + MAT;
-  double2* sG = sB + MAT;
-  double2* sAG = sG + MAT;
-  double2* sBG = sAG + MAT;
-  double2* tail = sBG + MAT;
-  GJScratch gs = carve_gj<NP, TG>(tail);
-  double* red = reinterpret_cast<double*>(reinterpret_cast<unsigned char*>(tail) + 3 * NP * 16 +
-                                          ((NP + 4) * 4 + 15) / 16 * 16);
+  // Roles rotate between iterations: pa = alpha, pb = beta, f0..f2 free,
+  // pes = eps_s (owner-only access).
+  double2* pa = reinterpret_cast<double2*>(smraw);
+  double2* pb = pa + MAT;
+  double2* f0 = pb + MAT;
+  double2* f1 = f0 + MAT;
+  double2* f2 = f1 + MAT;
+  double2* pes = f2 + MAT;
+  const GJShared gsh = carve_gj<NP>(reinterpret_cast<unsigned char*>(pes + MAT));
+  double* red = carve_red<NP>(pes + MAT);
 
   const int p = blockIdx.x;
   if (p >= a.batch) return;
   const int n = a.n;
-  const int tid = threadIdx.x, tr = tid / TG, tc = tid - tr * TG;
+  const int kch = (n + 7) >> 3;
+  const int tid = threadIdx.x;
+  const Lane L = lane_geo<NP>();
   const long long kset = a.kidx ? (long long)a.kidx[p] : 0;
   const double2* h00 = a.h00 + kset * a.lead_stride;
   const double2* h01 = a.h01 + kset * a.lead_stride;
@@ -274,72 +548,97 @@ __global__ void __launch_bounds__(TG* TG, 1) sr_f64_kernel(SrArgs a) {
   const double w = a.omega[p];
   const double2 z = z_of(w, a.eta[p]);
 
-  double2 eps[RT][RT], epss[RT][RT];
+  double2 eps[8];
 #pragma unroll
-  for (int i = 0; i < RT; ++i)
+  for (int j = 0; j < 2; ++j)
 #pragma unroll
-    for (int j = 0; j < RT; ++j) {
-      const int r = tr + TG * i, c = tc + TG * j;
-      double2 e = (r < n && c < n) ? h00[r * n + c] : make_double2(0.0, 0.0);
-      eps[i][j] = e;
-      epss[i][j] = e;
+    for (int q = 0; q < 4; ++q) {
+      const int r = own_r(L, q), c = own_c(L, j, q);
+      const double2 e = (r < n && c < n) ? h00[r * n + c] : make_double2(0.0, 0.0);
+      eps[j * 4 + q] = e;
+      pes[sidx<NP>(r, c)] = e;
     }
   for (int idx = tid; idx < NP * NP; idx += G::NTH) {
     const int r = idx / NP, c = idx - r * NP;
     const bool in = r < n && c < n;
-    sA[r * LD + c] = in ? h01[r * n + c] : make_double2(0.0, 0.0);
-    sB[r * LD + c] = in ? (h10 ? h10[r * n + c] : cconj(h01[c * n + r])) : make_double2(0.0, 0.0);
+    pa[sidx<NP>(r, c)] = in ? h01[r * n + c] : make_double2(0.0, 0.0);
+    pb[sidx<NP>(r, c)] = in ? (h10 ? h10[r * n + c] : cconj(h01[c * n + r])) : make_double2(0.0, 0.0);
   }
 
   int status = kOk;
   int it = 0;
   const double tol2 = a.tol * a.tol;
-  double2 c1[RT][RT], c2[RT][RT];
+  CAcc c1, c2;
   bool converged = false;
+  double2* pg = nullptr;
   for (it = 1; it <= a.maxiter; ++it) {
-    // M = z - eps (identity in the padding), inverted in place.
+    // M = z - eps (identity in the padding) into f0, inverted via f1.
 #pragma unroll
-    for (int i = 0; i < RT; ++i)
+    for (int j = 0; j < 2; ++j)
 #pragma unroll
-      for (int j = 0; j < RT; ++j) {
-        const int r = tr + TG * i, c = tc + TG * j;
+      for (int q = 0; q < 4; ++q) {
+        const int r = own_r(L, q), c = own_c(L, j, q);
         double2 v;
-        if (r < n && c < n) v = (r == c) ? csub(z, eps[i][j]) : cneg(eps[i][j]);
+        if (r < n && c < n) v = (r == c) ? csub(z, eps[j * 4 + q]) : cneg(eps[j * 4 + q]);
         else v = make_double2(r == c ? 1.0 : 0.0, 0.0);
-        sG[r * LD + c] = v;
+        f0[sidx<NP>(r, c)] = v;
       }
     __syncthreads();
-    status = gj_invert<NP, TG>(sG, n, gs);
+    status = gj_invert<NP>(f0, f1, f2, n, L, gsh, &pg);
     if (status != kOk) break;
+    double2* pag = (pg == f0) ? f1 : f0;  // the inversion's other buffer
+    double2* pbg = f2;
     // alpha g, beta g
-    mm2b<NP, TG>(c1, c2, sA, sB, sG, n, tr, tc);
-    store_tile<NP, TG>(sAG, c1, tr, tc);
-    store_tile<NP, TG>(sBG, c2, tr, tc);
+    cmm2b<NP>(c1, c2, pa, pb, pg, kch, L);
+    store_acc<NP>(pag, c1, L);
+    store_acc<NP>(pbg, c2, L);
     __syncthreads();
     // eps_s += (alpha g) beta ; eps += (alpha g) beta + (beta g) alpha
-    mmpair<NP, TG>(c1, c2, sAG, sB, sBG, sA, n, tr, tc);
     int bad = 0;
+    cmm<NP, false, false>(c1, pag, pb, kch, L);
 #pragma unroll
-    for (int i = 0; i < RT; ++i)
+    for (int j = 0; j < 2; ++j)
 #pragma unroll
-      for (int j = 0; j < RT; ++j) {
-        epss[i][j] = cadd(epss[i][j], c1[i][j]);
-        eps[i][j] = cadd(cadd(eps[i][j], c1[i][j]), c2[i][j]);
-        bad |= !cfinite(epss[i][j]) || !cfinite(eps[i][j]);
+      for (int q = 0; q < 4; ++q) {
+        const int e = sidx<NP>(own_r(L, q), own_c(L, j, q));
+        const double2 es = cadd(pes[e], c1.get(j, q));
+        pes[e] = es;
+        eps[j * 4 + q] = cadd(eps[j * 4 + q], c1.get(j, q));
+        bad |= !cfinite(es);
       }
-    // alpha <- (alpha g) alpha ; beta <- (beta g) beta
-    mmpair<NP, TG>(c1, c2, sAG, sA, sBG, sB, n, tr, tc);
+    cmm<NP, false, false>(c1, pbg, pa, kch, L);
+#pragma unroll
+    for (int j = 0; j < 2; ++j)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        eps[j * 4 + q] = cadd(eps[j * 4 + q], c1.get(j, q));
+        bad |= !cfinite(eps[j * 4 + q]);
+      }
+    // alpha' = (alpha g) alpha into the free g buffer ; beta' = (beta g) beta
     double e2 = 0.0;
+    cmm<NP, false, false>(c1, pag, pa, kch, L);
 #pragma unroll
-    for (int i = 0; i < RT; ++i)
+    for (int j = 0; j < 2; ++j)
 #pragma unroll
-      for (int j = 0; j < RT; ++j) {
-        bad |= !cfinite(c1[i][j]) || !cfinite(c2[i][j]);
-        e2 = fmax(e2, fmax(cabs2(c1[i][j]), cabs2(c2[i][j])));
+      for (int q = 0; q < 4; ++q) {
+        bad |= !cfinite(c1.get(j, q));
+        e2 = fmax(e2, cabs2(c1.get(j, q)));
+      }
+    store_acc<NP>(pg, c1, L);
+    cmm<NP, false, false>(c1, pbg, pb, kch, L);
+#pragma unroll
+    for (int j = 0; j < 2; ++j)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        bad |= !cfinite(c1.get(j, q));
+        e2 = fmax(e2, cabs2(c1.get(j, q)));
       }
     __syncthreads();  // every read of alpha and beta is done
-    store_tile<NP, TG>(sA, c1, tr, tc);
-    store_tile<NP, TG>(sB, c2, tr, tc);
+    store_acc<NP>(pb, c1, L);
+    f0 = pa;  // old alpha buffer is free
+    f1 = pag;
+    f2 = pbg;
+    pa = pg;
     if (block_any(bad)) { status = kNonFinite; break; }
     const double emax = block_max(e2, red);
     if (emax < tol2) { converged = true; break; }
@@ -350,30 +649,31 @@ __global__ void __launch_bounds__(TG* TG, 1) sr_f64_kernel(SrArgs a) {
   }
   if (status == kOk) {
 #pragma unroll
-    for (int i = 0; i < RT; ++i)
+    for (int j = 0; j < 2; ++j)
 #pragma unroll
-      for (int j = 0; j < RT; ++j) {
-        const int r = tr + TG * i, c = tc + TG * j;
+      for (int q = 0; q < 4; ++q) {
+        const int r = own_r(L, q), c = own_c(L, j, q);
+        const double2 es = pes[sidx<NP>(r, c)];
         double2 v;
-        if (r < n && c < n) v = (r == c) ? csub(z, epss[i][j]) : cneg(epss[i][j]);
+        if (r < n && c < n) v = (r == c) ? csub(z, es) : cneg(es);
         else v = make_double2(r == c ? 1.0 : 0.0, 0.0);
-        sG[r * LD + c] = v;
+        f0[sidx<NP>(r, c)] = v;
       }
     __syncthreads();
-    status = gj_invert<NP, TG>(sG, n, gs);
+    status = gj_invert<NP>(f0, f1, f2, n, L, gsh, &pg);
   }
   if (status == kOk) {
     if (a.g_out) {
       double2* go = a.g_out + (long long)p * n * n;
       for (int idx = tid; idx < n * n; idx += G::NTH) {
         const int r = idx / n, c = idx - r * n;
-        go[idx] = sG[r * LD + c];
+        go[idx] = pg[sidx<NP>(r, c)];
       }
     }
     if (a.dos_out) {
       // (omega/pi) Re Tr[i (g - g^H)] = (omega/pi) sum_j (-2 Im g_jj)
       double t = 0.0;
-      for (int j = tid; j < n; j += G::NTH) t += -2.0 * sG[j * LD + j].y;
+      for (int j = tid; j < n; j += G::NTH) t += -2.0 * pg[sidx<NP>(j, j)].y;
       t = block_sum(t, red);
       if (tid == 0) a.dos_out[p] = (w / 3.141592653589793238462643383279502884) * t;
     }
@@ -387,27 +687,29 @@ __global__ void __launch_bounds__(TG* TG, 1) sr_f64_kernel(SrArgs a) {
 }
 
 // ---------------------------------------------------------------- RGF sweep --
-template <int NP, int TG>
-__global__ void __launch_bounds__(TG* TG, 1) rgf_f64_kernel(RgfArgs a) {
-  using G = Geo<NP, TG>;
-  constexpr int RT = G::RT, LD = G::LD, MAT = G::MAT;
+// Shared buffers: pg (left-connected g_l) and pc (coupling / scratch) swap
+// roles with the inversion; bW = g_{l-1} C, bU = G_{0,l-1} C, bG0 = G_{0,l}.
+template <int NP>
+__global__ void __launch_bounds__(Geo<NP>::NTH, 1) rgf_f64_kernel(RgfArgs a) {
+  using G = Geo<NP>;
+  constexpr int MAT = G::MAT;
   extern __shared__ __align__(16) unsigned char smraw[];
-  double2* bG = reinterpret_cast<double2*>(smraw);  // left-connected g_i
-  double2* bC = bG + MAT;                             // coupling C_{i-1}
-  double2* bW = bC + MAT;                             // g_{i-1} C_{i-1}
-  double2* bU = bW + MAT;                             // G_{0,i-1} C_{i-1}
-  double2* bG0 = bU + MAT;                            // G_{0,i}
-  double2* tail = bG0 + MAT;
-  GJScratch gs = carve_gj<NP, TG>(tail);
-  double* red = reinterpret_cast<double*>(reinterpret_cast<unsigned char*>(tail) + 3 * NP * 16 +
-                                          ((NP + 4) * 4 + 15) / 16 * 16);
+  double2* const b0 = reinterpret_cast<double2*>(smraw);
+  double2* const b1 = b0 + MAT;
+  double2* const bW = b1 + MAT;
+  double2* const bU = bW + MAT;
+  double2* const bG0 = bU + MAT;
+  const GJShared gsh = carve_gj<NP>(reinterpret_cast<unsigned char*>(bG0 + MAT));
+  double* red = carve_red<NP>(bG0 + MAT);
   __shared__ int s_point;
 
   const int n = a.n, L = a.L;
-  const int tid = threadIdx.x, tr = tid / TG, tc = tid - tr * TG;
+  const int kch = (n + 7) >> 3;
+  const int tid = threadIdx.x;
+  const Lane Ln = lane_geo<NP>();
   double2* sigL = a.sigma_ws + (long long)blockIdx.x * 2 * n * n;
   double2* sigR = sigL + (long long)n * n;
-  double2 c1[RT][RT], c2[RT][RT];
+  CAcc c1, c2;
 
   for (;;) {
     if (tid == 0) s_point = (int)atomicAdd(a.counter, 1u);
@@ -427,36 +729,39 @@ __global__ void __launch_bounds__(TG* TG, 1) rgf_f64_kernel(RgfArgs a) {
     const double2 z = z_of(a.omega[p], a.eta_dev[p]);
     const double2* D = a.D + k * a.d_ks;
     const double2* C = a.C + k * a.c_ks;
+    double2* pg = b0;
+    double2* pc = b1;
 
     // Contact self-energies Sigma = V g V^H into this block's scratch.
     for (int side = 0; side < 2; ++side) {
       const int nl = side ? a.nr : a.nl;
+      const int lch = (nl + 7) >> 3;
       const double2* V = side ? a.VR + k * a.vr_ks : a.VL + k * a.vl_ks;
       const double2* g = side ? a.gR + (long long)p * a.gr_ps : a.gL + (long long)p * a.gl_ps;
       double2* S = side ? sigR : sigL;
-      load_mat<NP, TG>(bC, V, n, nl);
-      load_mat<NP, TG>(bW, g, nl, nl);
+      load_mat<NP>(pc, V, n, nl);
+      load_mat<NP>(bW, g, nl, nl);
       __syncthreads();
-      mm<NP, TG, false, false>(c1, bC, bW, nl, tr, tc);
-      store_tile<NP, TG>(bU, c1, tr, tc);
+      cmm<NP, false, false>(c1, pc, bW, lch, Ln);
+      store_acc<NP>(bU, c1, Ln);
       __syncthreads();
-      mm<NP, TG, false, true>(c1, bU, bC, nl, tr, tc);
+      cmm<NP, false, true>(c1, bU, pc, lch, Ln);
 #pragma unroll
-      for (int i = 0; i < RT; ++i)
+      for (int j = 0; j < 2; ++j)
 #pragma unroll
-        for (int j = 0; j < RT; ++j) {
-          const int r = tr + TG * i, c = tc + TG * j;
-          if (r < n && c < n) S[r * n + c] = c1[i][j];
+        for (int q = 0; q < 4; ++q) {
+          const int r = own_r(Ln, q), c = own_c(Ln, j, q);
+          if (r < n && c < n) S[r * n + c] = c1.get(j, q);
         }
       __syncthreads();
     }
 
     // Layer 0: g_0 = (z - D_0 - Sigma_L [- Sigma_R when L == 1])^-1 = G_{0,0}.
 #pragma unroll
-    for (int i = 0; i < RT; ++i)
+    for (int j = 0; j < 2; ++j)
 #pragma unroll
-      for (int j = 0; j < RT; ++j) {
-        const int r = tr + TG * i, c = tc + TG * j;
+      for (int q = 0; q < 4; ++q) {
+        const int r = own_r(Ln, q), c = own_c(Ln, j, q);
         double2 v;
         if (r < n && c < n) {
           v = csub(cneg(D[r * n + c]), sigL[r * n + c]);
@@ -465,51 +770,56 @@ __global__ void __launch_bounds__(TG* TG, 1) rgf_f64_kernel(RgfArgs a) {
         } else {
           v = make_double2(r == c ? 1.0 : 0.0, 0.0);
         }
-        bG[r * LD + c] = v;
+        pg[sidx<NP>(r, c)] = v;
       }
     __syncthreads();
-    int status = gj_invert<NP, TG>(bG, n, gs);
+    double2* inv = nullptr;
+    int status = gj_invert<NP>(pg, pc, bW, n, Ln, gsh, &inv);
     if (status == kOk) {
+      pc = (inv == pg) ? pc : pg;
+      pg = inv;
 #pragma unroll
-      for (int i = 0; i < RT; ++i)
+      for (int j = 0; j < 2; ++j)
 #pragma unroll
-        for (int j = 0; j < RT; ++j) {
-          const int r = tr + TG * i, c = tc + TG * j;
-          bG0[r * LD + c] = bG[r * LD + c];
+        for (int q = 0; q < 4; ++q) {
+          const int e = sidx<NP>(own_r(Ln, q), own_c(Ln, j, q));
+          bG0[e] = pg[e];
         }
       for (int l = 1; l < L && status == kOk; ++l) {
-        load_mat<NP, TG>(bC, C + (long long)(l - 1) * a.c_ls, n, n);
+        load_mat<NP>(pc, C + (long long)(l - 1) * a.c_ls, n, n);
         __syncthreads();
         // W = g_{l-1} C, U = G_{0,l-1} C
-        mm2b<NP, TG>(c1, c2, bG, bG0, bC, n, tr, tc);
-        store_tile<NP, TG>(bW, c1, tr, tc);
-        store_tile<NP, TG>(bU, c2, tr, tc);
+        cmm2b<NP>(c1, c2, pg, bG0, pc, kch, Ln);
+        store_acc<NP>(bW, c1, Ln);
+        store_acc<NP>(bU, c2, Ln);
         __syncthreads();
-        // M = z - D_l - C^H W [- Sigma_R on the last layer]
-        mm<NP, TG, true, false>(c1, bC, bW, n, tr, tc);
+        // M = z - D_l - C^H W [- Sigma_R on the last layer] into the old g buffer
+        cmm<NP, true, false>(c1, pc, bW, kch, Ln);
         const double2* Dl = D + (long long)l * a.d_ls;
         const bool last = (l == L - 1);
 #pragma unroll
-        for (int i = 0; i < RT; ++i)
+        for (int j = 0; j < 2; ++j)
 #pragma unroll
-          for (int j = 0; j < RT; ++j) {
-            const int r = tr + TG * i, c = tc + TG * j;
+          for (int q = 0; q < 4; ++q) {
+            const int r = own_r(Ln, q), c = own_c(Ln, j, q);
             double2 v;
             if (r < n && c < n) {
-              v = csub(cneg(Dl[r * n + c]), c1[i][j]);
+              v = csub(cneg(Dl[r * n + c]), c1.get(j, q));
               if (last) v = csub(v, sigR[r * n + c]);
               if (r == c) v = cadd(v, z);
             } else {
               v = make_double2(r == c ? 1.0 : 0.0, 0.0);
             }
-            bG[r * LD + c] = v;
+            pg[sidx<NP>(r, c)] = v;
           }
-        __syncthreads();
-        status = gj_invert<NP, TG>(bG, n, gs);
+        __syncthreads();  // C is dead once M is formed: pc becomes the second inversion buffer
+        status = gj_invert<NP>(pg, pc, bW, n, Ln, gsh, &inv);
         if (status != kOk) break;
+        pc = (inv == pg) ? pc : pg;
+        pg = inv;
         // G_{0,l} = U g_l
-        mm<NP, TG, false, false>(c1, bU, bG, n, tr, tc);
-        store_tile<NP, TG>(bG0, c1, tr, tc);
+        cmm<NP, false, false>(c1, bU, pg, kch, Ln);
+        store_acc<NP>(bG0, c1, Ln);
         __syncthreads();
       }
     }
@@ -517,10 +827,10 @@ __global__ void __launch_bounds__(TG* TG, 1) rgf_f64_kernel(RgfArgs a) {
     if (status == kOk) {
       // Gamma = i (Sigma - Sigma^H) for both contacts.
 #pragma unroll
-      for (int i = 0; i < RT; ++i)
+      for (int j = 0; j < 2; ++j)
 #pragma unroll
-        for (int j = 0; j < RT; ++j) {
-          const int r = tr + TG * i, c = tc + TG * j;
+        for (int q = 0; q < 4; ++q) {
+          const int r = own_r(Ln, q), c = own_c(Ln, j, q);
           double2 gl = make_double2(0.0, 0.0), gr = gl;
           if (r < n && c < n) {
             double2 d = csub(sigL[r * n + c], cconj(sigL[c * n + r]));
@@ -528,22 +838,21 @@ __global__ void __launch_bounds__(TG* TG, 1) rgf_f64_kernel(RgfArgs a) {
             d = csub(sigR[r * n + c], cconj(sigR[c * n + r]));
             gr = make_double2(-d.y, d.x);
           }
-          bC[r * LD + c] = gl;
-          bW[r * LD + c] = gr;
+          pc[sidx<NP>(r, c)] = gl;
+          bW[sidx<NP>(r, c)] = gr;
         }
       __syncthreads();
-      mm<NP, TG, false, false>(c1, bC, bG0, n, tr, tc);
-      store_tile<NP, TG>(bU, c1, tr, tc);
+      cmm<NP, false, false>(c1, pc, bG0, kch, Ln);
+      store_acc<NP>(bU, c1, Ln);
       __syncthreads();
-      mm<NP, TG, false, false>(c1, bU, bW, n, tr, tc);
+      cmm<NP, false, false>(c1, bU, bW, kch, Ln);
       double t = 0.0;
 #pragma unroll
-      for (int i = 0; i < RT; ++i)
+      for (int j = 0; j < 2; ++j)
 #pragma unroll
-        for (int j = 0; j < RT; ++j) {
-          const int r = tr + TG * i, c = tc + TG * j;
-          const double2 g = bG0[r * LD + c];
-          t += c1[i][j].x * g.x + c1[i][j].y * g.y;
+        for (int q = 0; q < 4; ++q) {
+          const double2 g = bG0[sidx<NP>(own_r(Ln, q), own_c(Ln, j, q))];
+          t += c1.re[j][q] * g.x + c1.im[j][q] * g.y;
         }
       tval = block_sum(t, red);
       if (!isfinite(tval)) status = kNonFinite;
@@ -687,50 +996,68 @@ __global__ void kappa_kernel(const double* __restrict__ om, const double* __rest
 }
 
 // ---------------------------------------------------------------- launchers --
-template <int NP, int TG>
-static size_t smem_bytes() { return (size_t)5 * Geo<NP, TG>::MAT * 16 + tail_bytes<NP>(); }
+template <int NP>
+static size_t smem_bytes() { return (size_t)5 * Geo<NP>::MAT * 16 + tail_bytes<NP>(); }
+template <int NP>
+static size_t sr_smem_bytes() { return (size_t)6 * Geo<NP>::MAT * 16 + tail_bytes<NP>(); }
 
-template <int NP, int TG>
+// Last launch failure of this host thread (read by the C-ABI layer).
+thread_local char g_launch_err[256] = "";
+
+template <typename K>
+static int record_failure(const char* what, K kernel, cudaError_t e, size_t smem, int threads) {
+  cudaFuncAttributes fa{};
+  cudaFuncGetAttributes(&fa, kernel);
+  snprintf(g_launch_err, sizeof(g_launch_err),
+           "%s: %s (threads %d, dynamic smem %zu, regs %d, max threads %d, static smem %zu)", what,
+           cudaGetErrorString(e), threads, smem, fa.numRegs, fa.maxThreadsPerBlock, fa.sharedSizeBytes);
+  return -3;
+}
+
+const char* last_launch_error() { return g_launch_err; }
+
+template <int NP>
 static int launch_sr(const SrArgs& a, cudaStream_t st) {
-  const size_t sm = smem_bytes<NP, TG>();
+  const size_t sm = sr_smem_bytes<NP>();
   static bool attr = false;
   if (!attr) {
-    if (cudaFuncSetAttribute(sr_f64_kernel<NP, TG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess)
-      return -3;
+    cudaError_t e = cudaFuncSetAttribute(sr_f64_kernel<NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return record_failure("sr_f64 smem attribute", sr_f64_kernel<NP>, e, sm, Geo<NP>::NTH);
     attr = true;
   }
-  sr_f64_kernel<NP, TG><<<a.batch, TG * TG, sm, st>>>(a);
-  return cudaGetLastError() == cudaSuccess ? 0 : -3;
+  sr_f64_kernel<NP><<<a.batch, Geo<NP>::NTH, sm, st>>>(a);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? 0 : record_failure("sr_f64 launch", sr_f64_kernel<NP>, e, sm, Geo<NP>::NTH);
 }
 
-template <int NP, int TG>
+template <int NP>
 static int launch_rgf(const RgfArgs& a, int grid, cudaStream_t st) {
-  const size_t sm = smem_bytes<NP, TG>();
+  const size_t sm = smem_bytes<NP>();
   static bool attr = false;
   if (!attr) {
-    if (cudaFuncSetAttribute(rgf_f64_kernel<NP, TG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess)
-      return -3;
+    cudaError_t e = cudaFuncSetAttribute(rgf_f64_kernel<NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return record_failure("rgf_f64 smem attribute", rgf_f64_kernel<NP>, e, sm, Geo<NP>::NTH);
     attr = true;
   }
-  rgf_f64_kernel<NP, TG><<<grid, TG * TG, sm, st>>>(a);
-  return cudaGetLastError() == cudaSuccess ? 0 : -3;
+  rgf_f64_kernel<NP><<<grid, Geo<NP>::NTH, sm, st>>>(a);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? 0 : record_failure("rgf_f64 launch", rgf_f64_kernel<NP>, e, sm, Geo<NP>::NTH);
 }
 
-template <int NP, int TG>
+template <int NP>
 static int occupancy_rgf() {
-  const size_t sm = smem_bytes<NP, TG>();
-  cudaFuncSetAttribute(rgf_f64_kernel<NP, TG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  const size_t sm = smem_bytes<NP>();
+  cudaFuncSetAttribute(rgf_f64_kernel<NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   int nb = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, rgf_f64_kernel<NP, TG>, TG * TG, sm) != cudaSuccess) return 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, rgf_f64_kernel<NP>, Geo<NP>::NTH, sm) != cudaSuccess)
+    return 0;
   return nb;
 }
 
-// Padded size for an order-n block: 1 (scalar path), 8, 16, 24, 32 or 48.
+// Padded size for an order-n block: 1 (scalar path), 16, 32 or 48.
 int padded_order(int n) {
   if (n == 1) return 1;
-  if (n <= 8) return 8;
   if (n <= 16) return 16;
-  if (n <= 24) return 24;
   if (n <= 32) return 32;
   if (n <= 48) return 48;
   return 0;
@@ -744,11 +1071,9 @@ int sr_f64_launch(const SrArgs& a, cudaStream_t st) {
       sr_scalar_kernel<<<(a.batch + tpb - 1) / tpb, tpb, 0, st>>>(a);
       return cudaGetLastError() == cudaSuccess ? 0 : -3;
     }
-    case 8: return launch_sr<8, 8>(a, st);
-    case 16: return launch_sr<16, 8>(a, st);
-    case 24: return launch_sr<24, 8>(a, st);
-    case 32: return launch_sr<32, 16>(a, st);
-    case 48: return launch_sr<48, 16>(a, st);
+    case 16: return launch_sr<16>(a, st);
+    case 32: return launch_sr<32>(a, st);
+    case 48: return launch_sr<48>(a, st);
     default: return -2;
   }
 }
@@ -760,11 +1085,9 @@ int rgf_f64_grid(int np) {
   int per = 0;
   switch (np) {
     case 1: return 0;
-    case 8: per = occupancy_rgf<8, 8>(); break;
-    case 16: per = occupancy_rgf<16, 8>(); break;
-    case 24: per = occupancy_rgf<24, 8>(); break;
-    case 32: per = occupancy_rgf<32, 16>(); break;
-    case 48: per = occupancy_rgf<48, 16>(); break;
+    case 16: per = occupancy_rgf<16>(); break;
+    case 32: per = occupancy_rgf<32>(); break;
+    case 48: per = occupancy_rgf<48>(); break;
     default: return -2;
   }
   return per > 0 ? per * nsm : -3;
@@ -778,11 +1101,9 @@ int rgf_f64_launch(const RgfArgs& a, int np, int grid, cudaStream_t st) {
       rgf_scalar_kernel<<<(a.batch + tpb - 1) / tpb, tpb, 0, st>>>(a);
       return cudaGetLastError() == cudaSuccess ? 0 : -3;
     }
-    case 8: return launch_rgf<8, 8>(a, grid, st);
-    case 16: return launch_rgf<16, 8>(a, grid, st);
-    case 24: return launch_rgf<24, 8>(a, grid, st);
-    case 32: return launch_rgf<32, 16>(a, grid, st);
-    case 48: return launch_rgf<48, 16>(a, grid, st);
+    case 16: return launch_rgf<16>(a, grid, st);
+    case 32: return launch_rgf<32>(a, grid, st);
+    case 48: return launch_rgf<48>(a, grid, st);
     default: return -2;
   }
 }
