@@ -98,6 +98,30 @@ int negf_rgf_transmission_f64(int n_dev, int n_lead_l, int n_lead_r, int n_layer
                               void* stream);
 
 /*
+ * Allocation-free form of negf_rgf_transmission_f64, for callers that cannot
+ * allocate device memory when they call (a host program that fixed its GPU
+ * memory budget and pools at start-up, or a binding from a language without
+ * a CUDA allocator).  It has no counterpart in negfpy.  Same arguments and
+ * outputs as negf_rgf_transmission_f64 without the workspace: the scratch
+ * lives in one static 16 MiB device array per GPU, held until the process
+ * exits.  The first call on a device looks up that array's device address
+ * (make it before any stream capture).  Calls share the array: calls whose
+ * GPU work overlaps race and must not be issued concurrently.  Returns
+ * NEGF_EUNSUPPORTED for block orders above 48 (the same limit as the
+ * allocating entry point; the persistent grid is capped to what fits the
+ * array), NEGF_EINVAL / NEGF_ECUDA as the other entry points.  Calls no
+ * allocator.
+ */
+int negf_rgf_transmission_f64_noalloc(int n_dev, int n_lead_l, int n_lead_r, int n_layers, int batch,
+                                      const double* onsite, long long onsite_kstride, long long onsite_lstride,
+                                      const double* coupling, long long coupling_kstride,
+                                      long long coupling_lstride, const double* v_left, long long v_left_kstride,
+                                      const double* v_right, long long v_right_kstride, const double* g_left,
+                                      long long g_left_pstride, const double* g_right, long long g_right_pstride,
+                                      const int* k_index, const double* omega, const double* eta_device,
+                                      const int* lead_status, double* t_out, int* status_out, void* stream);
+
+/*
  * k average of an omega-major [n_omega][n_k] transmission table.
  * Replaces the mean in negfpy core/negf.py:360-397 (transmission_kavg).
  */
