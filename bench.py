@@ -64,9 +64,10 @@ def _workload(rank: int, world: int, n_omega: int = N_OMEGA):
     ``n_omega`` < N_OMEGA keeps an evenly strided subset of the rank's shard
     (a profiling case with the same frequency distribution)."""
     from negfpy_b200 import workloads as W
+    from negfpy_b200.distributed import omega_shard
 
     wl = W.slab_workload(n_omega=N_OMEGA * world, n_k=N_K, n_layers=N_LAYERS)
-    shard = np.arange(rank, N_OMEGA * world, world)
+    shard = omega_shard(N_OMEGA * world, rank, world)
     if n_omega < N_OMEGA:
         shard = shard[:: max(1, N_OMEGA // n_omega)][:n_omega]
     return wl, shard
@@ -87,14 +88,23 @@ def _cpu_sample_pairs(wl, shard, n_points, seed=5):
     return [(int(a), int(b)) for a, b in zip(wi, ki)]
 
 
-def cpu_rate(wl, shard, n_points, cores):
-    """Oracle (negfpy's algorithm, SuperLU device solve) on a bounded sample; points/s."""
+def cpu_rate(wl, shard, n_points, cores, pool=None):
+    """Oracle (negfpy's algorithm, SuperLU device solve) on a bounded sample; points/s.
+
+    The pool is started and warmed (imports done) outside the timed region."""
     from oracle import negf_oracle as O
 
+    own = pool is None
+    if own:
+        pool = O.make_pool(cores)
+        O.transmission_points(wl, _cpu_sample_pairs(wl, shard, cores, seed=99), pool=pool)
     pairs = _cpu_sample_pairs(wl, shard, n_points)
     t0 = time.perf_counter()
-    O.transmission_points(wl, pairs, processes=cores)
+    O.transmission_points(wl, pairs, pool=pool)
     dt = time.perf_counter() - t0
+    if own:
+        pool.close()
+        pool.join()
     return n_points / dt, dt
 
 
@@ -170,13 +180,18 @@ def run_reference(args):
         return
     cores = os.cpu_count() or 1
     wl, shard = _workload(0, 1)
-    n = args.cpu_sample or max(4 * cores, 64)
-    if args.warmup > 0:  # one short untimed round starts the worker processes' imports
-        cpu_rate(wl, shard, min(n, 2 * cores), cores)
+    n = args.cpu_sample or max(16 * cores, 128)
+    from oracle import negf_oracle as O
+
+    pool = O.make_pool(cores)
+    for _ in range(max(args.warmup, 1)):  # untimed: worker start-up and imports
+        O.transmission_points(wl, _cpu_sample_pairs(wl, shard, cores, seed=99), pool=pool)
     rates = []
     for s in range(args.steps):
-        r, dt = cpu_rate(wl, shard, n, cores)
+        r, dt = cpu_rate(wl, shard, n, cores, pool=pool)
         rates.append(r)
+    pool.close()
+    pool.join()
     v = float(np.mean(rates))
     out = {
         "metric": METRIC, "value": v, "unit": "points/s", "n_gpus": ws, "steps": args.steps,
@@ -321,7 +336,7 @@ def main():
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cores = os.cpu_count() or 1
-        nsamp = args.cpu_sample or max(8 * cores, 64)
+        nsamp = args.cpu_sample or max(32 * cores, 256)
         rate, dt = cpu_rate(wl, shard, nsamp, cores)
         cpu = {"value": rate, "unit": "points/s", "cores": cores, "kind": "port",
                "sample": f"{nsamp} random points of the {W}x{K} grid ({dt:.1f} s wall); negfpy's algorithm "

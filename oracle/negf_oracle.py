@@ -227,8 +227,11 @@ def workload_point_args(wl, wi, ki):
                 idx_l=wl.meta.get("idx_l"), idx_r=wl.meta.get("idx_r"))
 
 
+_BLAS_VARS = ("OPENBLAS_NUM_THREADS", "OMP_NUM_THREADS", "MKL_NUM_THREADS")
+
+
 def _pool_init():
-    for v in ("OPENBLAS_NUM_THREADS", "OMP_NUM_THREADS", "MKL_NUM_THREADS"):
+    for v in _BLAS_VARS:
         os.environ[v] = "1"
 
 
@@ -239,17 +242,39 @@ def _pool_task(args):
         return float("nan")
 
 
-def transmission_points(wl, pairs, processes=1):
-    """T for a list of (omega_index, k_index) pairs; processes > 1 uses a spawn pool.
-
-    The pool mirrors negfpy's process backend (``workflows/ifc_bulk.py:1229-1253``)
-    with one BLAS thread per worker (``:621-670``).
-    """
-    args = [workload_point_args(wl, wi, ki) for wi, ki in pairs]
-    if processes <= 1:
-        return np.array([_pool_task(a) for a in args])
+def make_pool(processes):
+    """Spawn pool with one BLAS thread per worker, as negfpy's process backend
+    (``workflows/ifc_bulk.py:1229-1253``, ``:621-670``); spawn, not fork, so it
+    is safe to start after CUDA has been initialised."""
     import multiprocessing as mp
 
-    ctx = mp.get_context("spawn")
-    with ctx.Pool(processes, initializer=_pool_init) as pool:
-        return np.array(pool.map(_pool_task, args, chunksize=max(1, len(args) // (4 * processes))))
+    # Children inherit the environment at spawn, before numpy (and its BLAS)
+    # is imported in them, so the thread limit must be set here.
+    saved = {v: os.environ.get(v) for v in _BLAS_VARS}
+    for v in _BLAS_VARS:
+        os.environ[v] = "1"
+    try:
+        return mp.get_context("spawn").Pool(processes, initializer=_pool_init)
+    finally:
+        for v, old in saved.items():
+            if old is None:
+                os.environ.pop(v, None)
+            else:
+                os.environ[v] = old
+
+
+def transmission_points(wl, pairs, processes=1, pool=None):
+    """T for a list of (omega_index, k_index) pairs, serially or on a process pool."""
+    args = [workload_point_args(wl, wi, ki) for wi, ki in pairs]
+    if pool is None and processes <= 1:
+        return np.array([_pool_task(a) for a in args])
+    own = pool is None
+    if own:
+        pool = make_pool(processes)
+    try:
+        nproc = pool._processes
+        return np.array(pool.map(_pool_task, args, chunksize=max(1, len(args) // (4 * nproc))))
+    finally:
+        if own:
+            pool.close()
+            pool.join()
