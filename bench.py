@@ -307,6 +307,7 @@ def main():
     if tr_file.exists():
         tr = json.loads(tr_file.read_text())
         roof["traffic"] = tr.get(dom)
+        roof["traffic_source"] = "profiles/traffic.json (ncu, 4096-point case scaled to the launch)"
 
     # End to end through the public API: per-k block construction on the host,
     # upload, GPU solve, result back to host.
