@@ -45,8 +45,12 @@ int negf_get_version(void);
 /* Description of the last failing call on this host thread. */
 const char* negf_last_error(void);
 
-/* Largest block order the FP64 kernels accept. */
+/* Largest block order the FP64 kernels accept (orders up to 48 run from
+ * shared memory, 49..256 from a global-memory workspace). */
 int negf_max_order_f64(void);
+
+/* Workspace bytes negf_sgf_sr_f64 needs for block order n (0 on a bad size). */
+size_t negf_sgf_workspace_bytes(int n);
 
 /*
  * Batched Sancho-Rubio surface Green's function, FP64.
@@ -61,11 +65,13 @@ int negf_max_order_f64(void);
  *   dos_out[p]    (omega/pi) Re Tr[i (g - g^H)]
  *   iters_out[p]  decimation sweeps taken
  *   status_out[p] NEGF_OK / NEGF_MAXITER / NEGF_NONFINITE / NEGF_SINGULAR
+ * workspace: negf_sgf_workspace_bytes(n) bytes (a work counter, and the
+ * per-block matrices for n > 48); block orders 1..256.
  */
 int negf_sgf_sr_f64(int n, int batch, const double* h00, const double* h01, const double* h10,
                     long long lead_stride, const int* k_index, const double* omega, const double* eta,
                     double tol, int maxiter, double* g_out, double* dos_out, int* iters_out, int* status_out,
-                    void* stream);
+                    void* workspace, size_t workspace_bytes, void* stream);
 
 /* Workspace bytes negf_rgf_transmission_f64 needs (0 on a bad size). */
 size_t negf_rgf_workspace_bytes(int n_dev, int n_lead_l, int n_lead_r);

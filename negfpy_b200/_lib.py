@@ -30,7 +30,8 @@ _SIGNATURES = {
     "negf_get_version": (_I, []),
     "negf_last_error": (C.c_char_p, []),
     "negf_max_order_f64": (_I, []),
-    "negf_sgf_sr_f64": (_I, [_I, _I, _P, _P, _P, _LL, _P, _P, _P, _D, _I, _P, _P, _P, _P, _P]),
+    "negf_sgf_workspace_bytes": (_SZ, [_I]),
+    "negf_sgf_sr_f64": (_I, [_I, _I, _P, _P, _P, _LL, _P, _P, _P, _D, _I, _P, _P, _P, _P, _P, _SZ, _P]),
     "negf_rgf_workspace_bytes": (_SZ, [_I, _I, _I]),
     "negf_rgf_transmission_f64": (
         _I,

@@ -28,16 +28,26 @@ int negf_get_version(void) { return NEGF_B200_ABI_VERSION; }
 
 const char* negf_last_error(void) { return g_err; }
 
-int negf_max_order_f64(void) { return 48; }
+int negf_max_order_f64(void) { return 256; }
+
+size_t negf_sgf_workspace_bytes(int n) {
+  if (n <= 0 || n > 256) return 0;
+  if (n <= 48) return kCounterBytes;
+  const int np = negf::global_order(n);
+  const int grid = negf::sr_global_grid(np);
+  if (grid <= 0) return 0;
+  return kCounterBytes + negf::sr_global_ws_bytes(np, grid);
+}
 
 int negf_sgf_sr_f64(int n, int batch, const double* h00, const double* h01, const double* h10, long long lead_stride,
                     const int* k_index, const double* omega, const double* eta, double tol, int maxiter,
-                    double* g_out, double* dos_out, int* iters_out, int* status_out, void* stream) {
+                    double* g_out, double* dos_out, int* iters_out, int* status_out, void* workspace,
+                    size_t workspace_bytes, void* stream) {
   if (n <= 0 || batch < 0) return fail(NEGF_EINVAL, "negf_sgf_sr_f64: n must be positive and batch non-negative");
   if (!h00 || !h01 || !omega || !eta) return fail(NEGF_EINVAL, "negf_sgf_sr_f64: null input pointer");
   if (maxiter <= 0 || !(tol > 0.0)) return fail(NEGF_EINVAL, "negf_sgf_sr_f64: maxiter and tol must be positive");
   if (lead_stride < 0) return fail(NEGF_EINVAL, "negf_sgf_sr_f64: negative lead_stride");
-  if (negf::padded_order(n) == 0) return fail(NEGF_EUNSUPPORTED, "negf_sgf_sr_f64: block order above 48");
+  if (n > 256) return fail(NEGF_EUNSUPPORTED, "negf_sgf_sr_f64: block order above 256");
   negf::SrArgs a;
   a.n = n;
   a.batch = batch;
@@ -54,6 +64,22 @@ int negf_sgf_sr_f64(int n, int batch, const double* h00, const double* h01, cons
   a.dos_out = dos_out;
   a.iters_out = iters_out;
   a.status_out = status_out;
+  if (n > 48) {
+    const int np = negf::global_order(n);
+    const int grid = negf::sr_global_grid(np);
+    if (grid <= 0) return cuda_fail("negf_sgf_sr_f64: occupancy query");
+    if (!workspace || workspace_bytes < kCounterBytes + negf::sr_global_ws_bytes(np, grid))
+      return fail(NEGF_EINVAL, "negf_sgf_sr_f64: workspace missing or too small (see negf_sgf_workspace_bytes)");
+    if (batch == 0) return 0;
+    cudaStream_t st = as_stream(stream);
+    if (cudaMemsetAsync(workspace, 0, sizeof(unsigned int), st) != cudaSuccess)
+      return cuda_fail("negf_sgf_sr_f64: counter reset");
+    const int grc = negf::sr_f64_global_launch(a, np, grid,
+                                               reinterpret_cast<double2*>(static_cast<char*>(workspace) + kCounterBytes),
+                                               reinterpret_cast<unsigned*>(workspace), st);
+    if (grc != 0) return cuda_fail("negf_sgf_sr_f64 (global)");
+    return 0;
+  }
   int rc = negf::sr_f64_launch(a, as_stream(stream));
   if (rc == -2) return fail(NEGF_EUNSUPPORTED, "negf_sgf_sr_f64: block order not built");
   if (rc != 0) return fail(NEGF_ECUDA, negf::last_launch_error());
@@ -68,7 +94,15 @@ int rgf_grid_for(int np) { return np == 1 ? 0 : negf::rgf_f64_grid(np); }
 
 size_t negf_rgf_workspace_bytes(int n_dev, int n_lead_l, int n_lead_r) {
   if (n_dev <= 0 || n_lead_l <= 0 || n_lead_r <= 0) return 0;
-  const int np = negf::padded_order(max3(n_dev, n_lead_l, n_lead_r));
+  const int nmax = max3(n_dev, n_lead_l, n_lead_r);
+  if (nmax > 48) {
+    const int gp = negf::global_order(nmax);
+    if (gp == 0) return 0;
+    const int g = negf::rgf_global_grid(gp);
+    if (g <= 0) return 0;
+    return kCounterBytes + negf::rgf_global_ws_bytes(gp, n_dev, g);
+  }
+  const int np = negf::padded_order(nmax);
   if (np == 0) return 0;
   const int grid = rgf_grid_for(np);
   if (grid < 0) return 0;
@@ -91,11 +125,14 @@ int negf_rgf_transmission_f64(int n_dev, int n_lead_l, int n_lead_r, int n_layer
   if (onsite_kstride < 0 || onsite_lstride < 0 || coupling_kstride < 0 || coupling_lstride < 0 ||
       v_left_kstride < 0 || v_right_kstride < 0 || g_left_pstride < 0 || g_right_pstride < 0)
     return fail(NEGF_EINVAL, "negf_rgf_transmission_f64: negative stride");
-  const int np = negf::padded_order(max3(n_dev, n_lead_l, n_lead_r));
-  if (np == 0) return fail(NEGF_EUNSUPPORTED, "negf_rgf_transmission_f64: block order above 48");
-  const int grid = rgf_grid_for(np);
+  const int nmax = max3(n_dev, n_lead_l, n_lead_r);
+  const bool global = nmax > 48;
+  const int np = global ? negf::global_order(nmax) : negf::padded_order(nmax);
+  if (np == 0) return fail(NEGF_EUNSUPPORTED, "negf_rgf_transmission_f64: block order above 256");
+  const int grid = global ? negf::rgf_global_grid(np) : rgf_grid_for(np);
   if (grid < 0) return cuda_fail("negf_rgf_transmission_f64: occupancy query");
-  const size_t need = kCounterBytes + (size_t)grid * 2 * n_dev * n_dev * 16;
+  const size_t need = kCounterBytes + (global ? negf::rgf_global_ws_bytes(np, n_dev, grid)
+                                              : (size_t)grid * 2 * n_dev * n_dev * 16);
   if (!workspace || workspace_bytes < need)
     return fail(NEGF_EINVAL, "negf_rgf_transmission_f64: workspace missing or too small");
   if (batch == 0) return 0;
@@ -130,7 +167,7 @@ int negf_rgf_transmission_f64(int n_dev, int n_lead_l, int n_lead_r, int n_layer
   cudaStream_t st = as_stream(stream);
   if (np != 1 && cudaMemsetAsync(workspace, 0, sizeof(unsigned int), st) != cudaSuccess)
     return cuda_fail("negf_rgf_transmission_f64: counter reset");
-  int rc = negf::rgf_f64_launch(a, np, grid, st);
+  int rc = global ? negf::rgf_f64_global_launch(a, np, grid, a.sigma_ws, st) : negf::rgf_f64_launch(a, np, grid, st);
   if (rc == -2) return fail(NEGF_EUNSUPPORTED, "negf_rgf_transmission_f64: block order not built");
   if (rc != 0) return fail(NEGF_ECUDA, negf::last_launch_error());
   return 0;

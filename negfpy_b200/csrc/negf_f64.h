@@ -48,6 +48,15 @@ int sr_f64_launch(const SrArgs& a, cudaStream_t st);
 // Padded order np = padded_order(max(n, nl, nr)) selects the kernel variant.
 int rgf_f64_grid(int np);  // persistent grid size (blocks), 0 for the 1x1 path
 int rgf_f64_launch(const RgfArgs& a, int np, int grid, cudaStream_t st);
+// Block orders 49..256 (padded to a multiple of 16): global-memory workspace kernels.
+int global_order(int n);  // padded order for n > 48, 0 if unsupported
+int sr_global_grid(int np);
+int rgf_global_grid(int np);
+size_t sr_global_ws_bytes(int np, int grid);
+size_t rgf_global_ws_bytes(int np, int n, int grid);
+int sr_f64_global_launch(const SrArgs& a, int np, int grid, double2* ws, unsigned* counter, cudaStream_t st);
+int rgf_f64_global_launch(const RgfArgs& a, int np, int grid, double2* ws, cudaStream_t st);
+
 int kavg_launch(const double* T, int W, int K, double* tbar, cudaStream_t st);
 int kappa_launch(const double* om, const double* tbar, int W, const double* temps, int nT, double unit, double* out,
                  cudaStream_t st);

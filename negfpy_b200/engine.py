@@ -58,10 +58,14 @@ def sgf_sr(d00: torch.Tensor, d01: torch.Tensor, d10: torch.Tensor | None, omega
         return {"g": g, "dos": dos, "iters": iters, "status": status}
     if k_index is not None:
         k_index = k_index.to(device=dev, dtype=torch.int32).contiguous()
+    need = int(lib.negf_sgf_workspace_bytes(n))
+    if need == 0:
+        raise RuntimeError(f"block order {n} is not supported by the FP64 kernels")
+    ws = _workspace(need, dev, "sgf")
     rc = lib.negf_sgf_sr_f64(n, P, _lib.ptr(d00), _lib.ptr(d01), _lib.ptr(d10), n * n if K > 1 else 0,
                              _lib.ptr(k_index), _lib.ptr(omega), _lib.ptr(eta), float(tol), int(maxiter),
-                             _lib.ptr(g), _lib.ptr(dos), _lib.ptr(iters), _lib.ptr(status),
-                             _lib.stream_handle(stream))
+                             _lib.ptr(g), _lib.ptr(dos), _lib.ptr(iters), _lib.ptr(status), _lib.ptr(ws),
+                             ws.numel(), _lib.stream_handle(stream))
     _lib.check(rc, "negf_sgf_sr_f64")
     return {"g": g, "dos": dos, "iters": iters, "status": status}
 
@@ -69,8 +73,10 @@ def sgf_sr(d00: torch.Tensor, d01: torch.Tensor, d10: torch.Tensor | None, omega
 _ws_cache: dict = {}
 
 
-def _workspace(nbytes: int, dev: torch.device) -> torch.Tensor:
-    key = (dev.index,)
+def _workspace(nbytes: int, dev: torch.device, role: str = "rgf") -> torch.Tensor:
+    """Cached device workspace per (device, role); grown on demand.  Calls on
+    one stream reuse it safely (each launch resets its own work counter)."""
+    key = (dev.index, role)
     t = _ws_cache.get(key)
     if t is None or t.numel() < nbytes:
         t = torch.empty(max(nbytes, 256), dtype=torch.uint8, device=dev)

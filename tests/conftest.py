@@ -16,6 +16,11 @@ def pytest_configure(config):
 
 
 @pytest.fixture(scope="session")
+def golden_bulk():
+    return dict(np.load(GOLDEN / "bulk.npz"))
+
+
+@pytest.fixture(scope="session")
 def golden():
     return {name: dict(np.load(GOLDEN / f"{name}.npz")) for name in ("chain", "slab", "cases")}
 

@@ -85,6 +85,24 @@ def main() -> None:
                         eta=wl.eta, omega_max=wl.omega_max, g_pts=np.array(g_pts), g=g_slab, g_qep=g_slab_qep,
                         dos=dos_slab)
 
+    # ---- bulk (n = 96, L = 40): two k-points, a few omegas -------------------
+    wb = W.bulk_workload(n_k=16, n_omega=4096, n_layers=40)
+    kb = np.array([37, 170])
+    wb_sel = np.array([500, 1700, 2900])
+    tb, pairs_b = [], []
+    for ki in kb:
+        lb = LeadBlocks(d00=wb.lead_l["d00"][ki], d01=wb.lead_l["d01"][ki], d10=wb.lead_l["d10"][ki])
+        dv = Device1D(onsite_blocks=[wb.onsite[ki, 0]] * wb.n_layers,
+                      coupling_blocks=[wb.coupling[ki, 0]] * (wb.n_layers - 1))
+        for wi in wb_sel:
+            tb.append(R.transmission(float(wb.omegas[wi]), dv, lb, lb, eta=wb.eta))
+            pairs_b.append((wi, ki))
+    lb = LeadBlocks(d00=wb.lead_l["d00"][kb[0]], d01=wb.lead_l["d01"][kb[0]], d10=wb.lead_l["d10"][kb[0]])
+    gb = R.surface_gf(float(wb.omegas[1700]), lb.d00, lb.d01, lb.d10, eta=wb.eta)
+    np.savez_compressed(OUT / "bulk.npz", omegas=wb.omegas[wb_sel], wsel=wb_sel, ksel=kb, pairs=np.array(pairs_b),
+                        T=np.array(tb), d00=wb.lead_l["d00"][kb], d01=wb.lead_l["d01"][kb], n_layers=wb.n_layers,
+                        eta=wb.eta, g=gb)
+
     # ---- negfpy test-suite systems ----------------------------------------
     cases = {}
     # matched chain plateau, L = 20 (tests/test_chain_transmission.py)

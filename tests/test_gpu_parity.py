@@ -199,3 +199,62 @@ def test_inversion_against_numpy(n, scale):
     g = nb.surface_gf(0.7, d00, np.zeros((n, n)), eta=0.01)
     err = np.max(np.abs(g - ref)) / np.max(np.abs(ref))
     assert err <= 1e-12 * np.linalg.cond(m), err
+
+
+# ------------------------------------------------ block orders above 48 ----
+def test_bulk_n96_matches_reference(golden_bulk):
+    """n = 96, L = 40 (the bulk configuration): global-memory kernels vs negfpy."""
+    g = golden_bulk
+    L = int(g["n_layers"])
+    ts = []
+    for wi, ki in g["pairs"]:
+        j = int(np.where(g["ksel"] == ki)[0][0])
+        w = float(g["omegas"][np.where(g["wsel"] == wi)[0][0]])
+        d00, d01 = g["d00"][j], g["d01"][j]
+        lead = nb.LeadBlocks(d00=d00, d01=d01, d10=np.conj(d01).T)
+        dev = nb.Device1D([d00] * L, [d01] * (L - 1))
+        ts.append(nb.transmission(w, dev, lead, lead, eta=float(g["eta"])))
+    assert rel_err(ts, g["T"]).max() <= TOL_T
+    w = float(g["omegas"][np.where(g["wsel"] == 1700)[0][0]])
+    gs = nb.surface_gf(w, g["d00"][0], g["d01"][0], np.conj(g["d01"][0]).T, eta=float(g["eta"]))
+    assert np.max(np.abs(gs - g["g"])) <= 1e-10 * np.max(np.abs(g["g"]))
+
+
+@pytest.mark.parametrize("n", [49, 64, 96, 150, 192])
+def test_inversion_large_orders_against_numpy(n):
+    rng = np.random.default_rng(n)
+    d00 = rng.normal(size=(n, n)) + 1j * rng.normal(size=(n, n))
+    z = (0.7 + 1j * 0.01) ** 2
+    m = z * np.eye(n) - d00
+    ref = np.linalg.inv(m)
+    g = nb.surface_gf(0.7, d00, np.zeros((n, n)), eta=0.01)
+    err = np.max(np.abs(g - ref)) / np.max(np.abs(ref))
+    assert err <= 1e-12 * np.linalg.cond(m), err
+
+
+def test_mixed_orders_heterojunction_vs_oracle():
+    """Left lead n = 48, right lead n = 72, device blocks of order 72 with the
+    left contact on the first 48 DOFs (rectangular couplings, explicit contact
+    indices), against the CPU oracle."""
+    left = W.spring_network(21, ny=2, nz=8, periodic_y=True)
+    right = W.spring_network(22, ny=3, nz=8, periodic_y=True, spring_range=(0.8, 1.6), mass_range=(0.9, 1.4))
+    from negfpy_b200.models import material_kspace_stack
+
+    kp = [(0.4,)]
+    sl = material_kspace_stack(left, kp)
+    sr = material_kspace_stack(right, kp, n_layers=5)
+    L = 5
+    on = [sr["onsite"][0, i] for i in range(L)]
+    cp = [sr["coupling"][0, i] for i in range(L - 1)]
+    ll = (sl["d00"][0], sl["d01"][0], sl["d10"][0])
+    lr = (sr["d00"][0], sr["d01"][0], sr["d10"][0])
+    vl = np.zeros((48, 48), dtype=complex)
+    vl[:, :] = 0.8 * sl["d10"][0]
+    idx_l = list(range(48))
+    idx_r = list(range(72 * (L - 1), 72 * L))
+    for w in (0.9, 1.7, 2.6):
+        ref = O.transmission_point(w, on, cp, ll, lr, eta=1e-4, vl=vl, vr=lr[1], idx_l=idx_l, idx_r=idx_r)
+        t = nb.transmission(w, nb.Device1D(on, cp), nb.LeadBlocks(*ll), nb.LeadBlocks(*lr), eta=1e-4,
+                            device_to_lead_left=vl, device_to_lead_right=lr[1], contact_left_indices=idx_l,
+                            contact_right_indices=idx_r)
+        assert rel_err(t, ref) <= TOL_T, (w, t, ref)

@@ -83,3 +83,16 @@ def test_oracle_error_cases():
     # exactly singular decimation block
     with pytest.raises(np.linalg.LinAlgError):
         O.sancho_rubio(1.0, np.eye(3), np.zeros((3, 3)), None, 0.0)
+
+
+def test_bulk_n96_oracle_matches_reference():
+    g = dict(np.load(__import__("tests.conftest", fromlist=["GOLDEN"]).GOLDEN / "bulk.npz"))
+    L = int(g["n_layers"])
+    for i in (0, 4):
+        wi, ki = g["pairs"][i]
+        j = int(np.where(g["ksel"] == ki)[0][0])
+        w = float(g["omegas"][np.where(g["wsel"] == wi)[0][0]])
+        d00, d01 = g["d00"][j], g["d01"][j]
+        lead = (d00, d01, np.conj(d01).T)
+        t = O.transmission_point(w, [d00] * L, [d01] * (L - 1), lead, lead, eta=float(g["eta"]))
+        assert rel_err(t, g["T"][i]) < 1e-11
