@@ -127,6 +127,32 @@ int negf_rgf_transmission_f64_noalloc(int n_dev, int n_lead_l, int n_lead_r, int
                                       const int* k_index, const double* omega, const double* eta_device,
                                       const int* lead_status, double* t_out, int* status_out, void* stream);
 
+/* Workspace bytes negf_rgf_adjoint_f64 needs (0 on a bad size). */
+size_t negf_adjoint_workspace_bytes(int n_dev, int n_lead_l, int n_lead_r, int n_layers);
+
+/*
+ * Adjoint of the device solve, FP64 (no counterpart in negfpy, which has no
+ * derivatives; it differentiates core/negf.py:306-357 with respect to the
+ * device blocks).  Same inputs as negf_rgf_transmission_f64 plus weight[p]
+ * (e.g. dkappa/dT of the point).  With G = A^-1, Y = Gamma_R G_{0,L-1}^H
+ * Gamma_L and X_ji = G_{j,L-1} Y G_{0,i}, it ADDS, for the point's k:
+ *   grad_onsite[k][i]   += weight[p] X_ii                  ([K][L][n][n])
+ *   grad_coupling[k][i] += weight[p] (X_{i+1,i} + X_{i,i+1}^H)   ([K][L-1][n][n])
+ * so that dT = 2 Re sum_i Tr[dD_i X_ii] + 2 Re sum_i Tr[dC_i (...)].  The
+ * caller zeroes the accumulators.  T and status as negf_rgf_transmission_f64;
+ * nothing is kept between calls (the forward sweeps are recomputed).
+ * Block orders 1..256.
+ */
+int negf_rgf_adjoint_f64(int n_dev, int n_lead_l, int n_lead_r, int n_layers, int batch, const double* onsite,
+                         long long onsite_kstride, long long onsite_lstride, const double* coupling,
+                         long long coupling_kstride, long long coupling_lstride, const double* v_left,
+                         long long v_left_kstride, const double* v_right, long long v_right_kstride,
+                         const double* g_left, long long g_left_pstride, const double* g_right,
+                         long long g_right_pstride, const int* k_index, const double* omega,
+                         const double* eta_device, const int* lead_status, const double* weight, double* grad_onsite,
+                         double* grad_coupling, double* t_out, int* status_out, void* workspace,
+                         size_t workspace_bytes, void* stream);
+
 /*
  * k average of an omega-major [n_omega][n_k] transmission table.
  * Replaces the mean in negfpy core/negf.py:360-397 (transmission_kavg).

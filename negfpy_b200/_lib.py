@@ -43,6 +43,12 @@ _SIGNATURES = {
         [_I, _I, _I, _I, _I, _P, _LL, _LL, _P, _LL, _LL, _P, _LL, _P, _LL, _P, _LL, _P, _LL, _P, _P, _P, _P, _P,
          _P, _P],
     ),
+    "negf_adjoint_workspace_bytes": (_SZ, [_I, _I, _I, _I]),
+    "negf_rgf_adjoint_f64": (
+        _I,
+        [_I, _I, _I, _I, _I, _P, _LL, _LL, _P, _LL, _LL, _P, _LL, _P, _LL, _P, _LL, _P, _LL, _P, _P, _P, _P, _P,
+         _P, _P, _P, _P, _P, _SZ, _P],
+    ),
     "negf_kavg_f64": (_I, [_P, _I, _I, _P, _P]),
     "negf_kappa_f64": (_I, [_P, _P, _I, _P, _I, _D, _P, _P]),
 }

@@ -42,6 +42,15 @@ struct RgfArgs {
   unsigned int* counter;    // zeroed work counter
 };
 
+// Adjoint of the device solve: RgfArgs plus per-point weights and the
+// per-k accumulators of the adjoint blocks.
+struct GradArgs {
+  RgfArgs r;
+  const double* weight;  // [batch] dKappa/dT of each point
+  double2* grad_d;       // [K][L][n][n]    += weight X_ii
+  double2* grad_c;       // [K][L-1][n][n]  += weight (X_{i+1,i} + X_{i,i+1}^H)
+};
+
 int padded_order(int n);
 const char* last_launch_error();  // message of the last failed launch on this thread
 int sr_f64_launch(const SrArgs& a, cudaStream_t st);
@@ -56,6 +65,10 @@ size_t sr_global_ws_bytes(int np, int grid);
 size_t rgf_global_ws_bytes(int np, int n, int grid);
 int sr_f64_global_launch(const SrArgs& a, int np, int grid, double2* ws, unsigned* counter, cudaStream_t st);
 int rgf_f64_global_launch(const RgfArgs& a, int np, int grid, double2* ws, cudaStream_t st);
+
+size_t grad_ws_bytes(int np, int n, int L, int grid);
+int grad_grid(int np);
+int grad_f64_launch(const GradArgs& ga, int np, int grid, double2* ws, cudaStream_t st);
 
 int kavg_launch(const double* T, int W, int K, double* tbar, cudaStream_t st);
 int kappa_launch(const double* om, const double* tbar, int W, const double* temps, int nT, double unit, double* out,

@@ -694,6 +694,253 @@ __global__ void __launch_bounds__(kThreads) rgf_f64_global_kernel(RgfArgs a, int
   }
 }
 
+// ------------------------------------------------------- adjoint (gradient) --
+// Whole-matrix helpers over the (NP/16)^2 tiles of a block (each ends with a
+// barrier).
+template <bool AC, bool BC>
+__device__ void gemm_to(double2* dst, const double2* A, const double2* B, int NP, int kch) {
+  const int warp = threadIdx.x >> 5, np16 = NP >> 4, nt = np16 * np16;
+  for (int tt = warp; tt < nt; tt += kWarps) {
+    const Tile T = tile_of(tt, np16);
+    Acc c;
+    tile_mm<AC, BC>(c, A, NP, B, NP, kch, T);
+#pragma unroll
+    for (int j = 0; j < 2; ++j)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) dst[(long long)tr(T, q) * NP + tc(T, j, q)] = c.get(j, q);
+  }
+  __syncthreads();
+}
+// dst = z - D - op(A) op(B) [- S1] [- S2] on the leading n x n block, identity
+// padding; A == nullptr drops the product.
+template <bool AC, bool BC>
+__device__ void form_m(double2* dst, const double2* A, const double2* B, const double2* __restrict__ D,
+                       const double2* S1, const double2* S2, double2 z, int n, int NP, int kch) {
+  const int warp = threadIdx.x >> 5, np16 = NP >> 4, nt = np16 * np16;
+  for (int tt = warp; tt < nt; tt += kWarps) {
+    const Tile T = tile_of(tt, np16);
+    Acc c;
+    if (A) tile_mm<AC, BC>(c, A, NP, B, NP, kch, T);
+    else c.zero();
+#pragma unroll
+    for (int j = 0; j < 2; ++j)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int r = tr(T, q), cc = tc(T, j, q);
+        double2 v;
+        if (r < n && cc < n) {
+          v = csub(cneg(D[r * n + cc]), c.get(j, q));
+          if (S1) v = csub(v, S1[r * n + cc]);
+          if (S2) v = csub(v, S2[r * n + cc]);
+          if (r == cc) v = cadd(v, z);
+        } else {
+          v = make_double2(r == cc ? 1.0 : 0.0, 0.0);
+        }
+        dst[(long long)r * NP + cc] = v;
+      }
+  }
+  __syncthreads();
+}
+__device__ void copy_mat(double2* dst, const double2* src, int NP) {
+  for (long long e = threadIdx.x; e < (long long)NP * NP; e += kThreads) dst[e] = src[e];
+  __syncthreads();
+}
+// Inverse of the matrix formed in `slot`, left in `slot` (Y is scratch).
+__device__ int invert_into(double2* slot, double2* Y, int n, int NP, const GJS& sh) {
+  double2* out = nullptr;
+  const int st = gj_invert_global(slot, Y, n, NP, sh, &out);
+  if (st == kOk && out != slot) copy_mat(slot, out, NP);
+  return st;
+}
+__device__ __forceinline__ void atomic_cadd(double2* dst, double2 v) {
+  atomicAdd(&dst->x, v.x);
+  atomicAdd(&dst->y, v.y);
+}
+
+// Per point: T and the weighted adjoint blocks of dT/dD.  With G = A^-1 for
+// A = z - D - Sigma_L - Sigma_R, Y = Gamma_R G_{0,L-1}^H Gamma_L and
+// X_{ji} = G_{j,L-1} Y G_{0,i},
+//     dT = 2 Re sum_ij Tr[dD_ij X_ji],
+// so a change dD_i of onsite block i contributes 2 Re Tr[dD_i X_ii] and a
+// change dC_i of the coupling between layers i and i+1 (with dC_i^H below the
+// diagonal) contributes 2 Re Tr[dC_i (X_{i+1,i} + X_{i,i+1}^H)].  The kernel
+// adds weight[p] X_ii into grad_d[k][i] and weight[p] (X_{i+1,i} + X_{i,i+1}^H)
+// into grad_c[k][i].  Nothing is kept from the forward pass: the left sweep
+// (g^L), the last block column G_{j,L-1} (backward recursion), the right sweep
+// (g^R) and the first block row G_{0,i} are recomputed here, per point.
+__global__ void __launch_bounds__(kThreads) rgf_grad_f64_kernel(GradArgs ga, int NP, double2* ws) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const GJS sh = carve(smraw, NP);
+  double* red = reinterpret_cast<double*>(smraw + ((gjs_bytes(NP) + 15) / 16) * 16);
+  __shared__ int s_point;
+  const RgfArgs& a = ga.r;
+  const int n = a.n, L = a.L, tid = threadIdx.x;
+  const int kch = (n + 7) >> 3;
+  const long long M2 = (long long)NP * NP;
+  double2* base = ws + (long long)blockIdx.x * ((14 + 2LL * L) * M2 + 2LL * n * n);
+  double2* B[14];
+  for (int i = 0; i < 14; ++i) B[i] = base + i * M2;
+  double2* gl = base + 14 * M2;             // L slots: g^L_j, then G_{j,L-1}
+  double2* gr = gl + (long long)L * M2;     // L slots: g^R_i
+  double2* sigL = gr + (long long)L * M2;
+  double2* sigR = sigL + (long long)n * n;
+  double2 *Cb = B[0], *W = B[1], *Mb = B[2], *Xs = B[3], *GL = B[4], *GR = B[5], *Y = B[6];
+  double2 *Ap = B[7], *Ac = B[8], *G0p = B[9], *G0c = B[10], *Xa = B[11], *Xb = B[12], *Tt = B[13];
+
+  for (;;) {
+    if (tid == 0) s_point = (int)atomicAdd(a.counter, 1u);
+    __syncthreads();
+    const int p = s_point;
+    __syncthreads();
+    if (p >= a.batch) break;
+    const int lst = a.lead_status ? a.lead_status[p] : 0;
+    if (lst != kOk) {
+      if (tid == 0) {
+        a.T_out[p] = __longlong_as_double(0x7ff8000000000000ULL);
+        if (a.status_out) a.status_out[p] = lst;
+      }
+      continue;
+    }
+    const long long k = a.kidx ? (long long)a.kidx[p] : 0;
+    const double2 z = z_of(a.omega[p], a.eta_dev[p]);
+    const double2* D = a.D + k * a.d_ks;
+    const double2* C = a.C + k * a.c_ks;
+    const double wgt = ga.weight[p];
+    double2* gdk = ga.grad_d + k * (long long)L * n * n;
+    double2* gck = ga.grad_c + k * (long long)(L > 1 ? L - 1 : 1) * n * n;
+    auto Dl = [&](int l) { return D + (long long)l * a.d_ls; };
+    auto load_c = [&](int l) {
+      load_pad(Cb, C + (long long)l * a.c_ls, n, n, NP, 0.0);
+      __syncthreads();
+    };
+
+    // Sigma and Gamma of both contacts.
+    for (int side = 0; side < 2; ++side) {
+      const int nl = side ? a.nr : a.nl;
+      const int lch = (nl + 7) >> 3;
+      const double2* V = side ? a.VR + k * a.vr_ks : a.VL + k * a.vl_ks;
+      const double2* g = side ? a.gR + (long long)p * a.gr_ps : a.gL + (long long)p * a.gl_ps;
+      double2* S = side ? sigR : sigL;
+      load_pad(W, V, n, nl, NP, 0.0);
+      load_pad(Xs, g, nl, nl, NP, 0.0);
+      __syncthreads();
+      gemm_to<false, false>(Tt, W, Xs, NP, lch);
+      gemm_to<false, true>(Mb, Tt, W, NP, lch);
+      for (long long e = tid; e < M2; e += kThreads) {
+        const int r = (int)(e / NP), c = (int)(e - (long long)r * NP);
+        if (r < n && c < n) S[r * n + c] = Mb[e];
+      }
+      __syncthreads();
+    }
+    for (long long e = tid; e < M2; e += kThreads) {
+      const int r = (int)(e / NP), c = (int)(e - (long long)r * NP);
+      double2 gl_ = make_double2(0.0, 0.0), gr_ = gl_;
+      if (r < n && c < n) {
+        double2 d = csub(sigL[r * n + c], cconj(sigL[c * n + r]));
+        gl_ = make_double2(-d.y, d.x);
+        d = csub(sigR[r * n + c], cconj(sigR[c * n + r]));
+        gr_ = make_double2(-d.y, d.x);
+      }
+      GL[e] = gl_;
+      GR[e] = gr_;
+    }
+    __syncthreads();
+
+    int status = kOk;
+    // 1. left sweep: gl[l] = g^L_l
+    form_m<false, false>(gl, nullptr, nullptr, Dl(0), sigL, L == 1 ? sigR : nullptr, z, n, NP, kch);
+    status = invert_into(gl, Xs, n, NP, sh);
+    for (int l = 1; l < L && status == kOk; ++l) {
+      load_c(l - 1);
+      gemm_to<false, false>(W, gl + (l - 1) * M2, Cb, NP, kch);
+      form_m<true, false>(gl + l * M2, Cb, W, Dl(l), l == L - 1 ? sigR : nullptr, nullptr, z, n, NP, kch);
+      status = invert_into(gl + l * M2, Xs, n, NP, sh);
+    }
+    // 2. last block column: G_{L-1,L-1} = g^L_{L-1}, G_{j,L-1} = g^L_j C_j G_{j+1,L-1}
+    for (int j = L - 2; j >= 0 && status == kOk; --j) {
+      load_c(j);
+      gemm_to<false, false>(W, Cb, gl + (j + 1) * M2, NP, kch);
+      gemm_to<false, false>(Tt, gl + j * M2, W, NP, kch);
+      copy_mat(gl + j * M2, Tt, NP);
+    }
+    double tval = 0.0;
+    if (status == kOk) {
+      // T = Re Tr[Gamma_L G Gamma_R G^H], G = G_{0,L-1};  Y = Gamma_R G^H Gamma_L
+      gemm_to<false, false>(Tt, GL, gl, NP, kch);
+      gemm_to<false, false>(W, Tt, GR, NP, kch);
+      double t = 0.0;
+      for (long long e = tid; e < M2; e += kThreads) t += W[e].x * gl[e].x + W[e].y * gl[e].y;
+      tval = block_sum(t, red);
+      if (!isfinite(tval)) status = kNonFinite;
+      gemm_to<true, false>(Tt, gl, GL, NP, kch);
+      gemm_to<false, false>(Y, GR, Tt, NP, kch);
+    }
+    // 3. right sweep: gr[i] = g^R_i, then G_{0,0}
+    if (status == kOk) {
+      form_m<false, false>(gr + (L - 1) * M2, nullptr, nullptr, Dl(L - 1), sigR, L == 1 ? sigL : nullptr, z, n, NP,
+                           kch);
+      status = invert_into(gr + (L - 1) * M2, Xs, n, NP, sh);
+      for (int i = L - 2; i >= 1 && status == kOk; --i) {
+        load_c(i);
+        gemm_to<false, false>(W, Cb, gr + (i + 1) * M2, NP, kch);
+        form_m<false, true>(gr + i * M2, W, Cb, Dl(i), nullptr, nullptr, z, n, NP, kch);
+        status = invert_into(gr + i * M2, Xs, n, NP, sh);
+      }
+      if (status == kOk) {
+        if (L == 1) {
+          copy_mat(G0c, gr, NP);
+        } else {
+          load_c(0);
+          gemm_to<false, false>(W, Cb, gr + M2, NP, kch);
+          form_m<false, true>(G0c, W, Cb, Dl(0), sigL, nullptr, z, n, NP, kch);
+          status = invert_into(G0c, Xs, n, NP, sh);
+        }
+      }
+    }
+    // 4. first block row and the adjoint blocks
+    for (int i = 0; i < L && status == kOk; ++i) {
+      gemm_to<false, false>(Ac, gl + i * M2, Y, NP, kch);
+      gemm_to<false, false>(Xa, Ac, G0c, NP, kch);
+      for (long long e = tid; e < M2; e += kThreads) {
+        const int r = (int)(e / NP), c = (int)(e - (long long)r * NP);
+        if (r < n && c < n) {
+          const double2 v = Xa[e];
+          atomic_cadd(gdk + (long long)i * n * n + r * n + c, make_double2(wgt * v.x, wgt * v.y));
+        }
+      }
+      __syncthreads();  // Xa is rewritten next
+      if (i >= 1) {
+        gemm_to<false, false>(Xa, Ac, G0p, NP, kch);   // X_{i,i-1}
+        gemm_to<false, false>(Xb, Ap, G0c, NP, kch);   // X_{i-1,i}
+        for (long long e = tid; e < M2; e += kThreads) {
+          const int r = (int)(e / NP), c = (int)(e - (long long)r * NP);
+          if (r < n && c < n) {
+            const double2 v = cadd(Xa[e], cconj(Xb[(long long)c * NP + r]));
+            atomic_cadd(gck + (long long)(i - 1) * n * n + r * n + c, make_double2(wgt * v.x, wgt * v.y));
+          }
+        }
+      }
+      if (i + 1 < L) {
+        load_c(i);
+        gemm_to<false, false>(Tt, G0c, Cb, NP, kch);
+        gemm_to<false, false>(G0p, Tt, gr + (i + 1) * M2, NP, kch);  // G_{0,i+1} into the spare buffer
+        double2* t = G0p;
+        G0p = G0c;
+        G0c = t;
+        t = Ap;
+        Ap = Ac;
+        Ac = t;
+      }
+    }
+    __syncthreads();
+    if (tid == 0) {
+      a.T_out[p] = (status == kOk) ? tval : __longlong_as_double(0x7ff8000000000000ULL);
+      if (a.status_out) a.status_out[p] = status;
+    }
+    __syncthreads();
+  }
+}
+
 // ---------------------------------------------------------------- launchers --
 size_t smem_bytes(int np) { return ((gjs_bytes(np) + 15) / 16) * 16 + 40 * 8; }
 
@@ -718,6 +965,22 @@ size_t rgf_global_ws_bytes(int np, int n, int grid) { return (size_t)grid * (6 *
 int sr_f64_global_launch(const SrArgs& a, int np, int grid, double2* ws, unsigned* counter, cudaStream_t st) {
   if (a.batch <= 0) return 0;
   glob::sr_f64_global_kernel<<<grid, glob::kThreads, glob::smem_bytes(np), st>>>(a, np, ws, counter);
+  return cudaGetLastError() == cudaSuccess ? 0 : -3;
+}
+
+size_t grad_ws_bytes(int np, int n, int L, int grid) {
+  return (size_t)grid * ((14 + 2 * (size_t)L) * np * np + 2 * (size_t)n * n) * 16;
+}
+int grad_grid(int np) {
+  const int g = glob::occupancy_grid(glob::rgf_grad_f64_kernel, np);
+  int dev = 0, nsm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  return g > nsm ? nsm : g;  // one block per SM bounds the 2L-slot workspace
+}
+int grad_f64_launch(const GradArgs& ga, int np, int grid, double2* ws, cudaStream_t st) {
+  if (ga.r.batch <= 0) return 0;
+  glob::rgf_grad_f64_kernel<<<grid, glob::kThreads, glob::smem_bytes(np), st>>>(ga, np, ws);
   return cudaGetLastError() == cudaSuccess ? 0 : -3;
 }
 

@@ -123,6 +123,49 @@ def rgf_transmission(onsite: torch.Tensor, coupling: torch.Tensor | None, n_laye
     return T, st
 
 
+def rgf_adjoint(onsite: torch.Tensor, coupling: torch.Tensor, n_layers: int, vl: torch.Tensor, vr: torch.Tensor,
+                gl: torch.Tensor, gr: torch.Tensor, omega: torch.Tensor, eta_dev: torch.Tensor,
+                k_index: torch.Tensor, lead_status: torch.Tensor | None, weight: torch.Tensor,
+                stream=None) -> tuple[torch.Tensor, torch.Tensor, torch.Tensor, torch.Tensor]:
+    """Vector-Jacobian product of T with respect to the device blocks.
+
+    Layer-resolved blocks ``onsite`` ``[K, L, n, n]`` and ``coupling`` ``[K, L-1, n, n]``
+    (no stride-0 sharing: every block is a variable).  Returns (T, status,
+    grad_onsite, grad_coupling) with sum_p weight[p] dT_p = 2 Re sum Tr[dD X]
+    over the returned adjoint blocks (``negf_rgf_adjoint_f64``)."""
+    lib = _lib.load()
+    dev = _dev()
+    K, L, n, _ = onsite.shape
+    if L != n_layers:
+        raise ValueError("rgf_adjoint needs one onsite block per layer")
+    nl, nr = int(vl.shape[-1]), int(vr.shape[-1])
+    P = int(omega.shape[0])
+    T = torch.empty(P, dtype=RDT, device=dev)
+    st = torch.empty(P, dtype=torch.int32, device=dev)
+    g_on = torch.zeros((K, L, n, n), dtype=CDT, device=dev)
+    g_cp = torch.zeros((K, max(L - 1, 1), n, n), dtype=CDT, device=dev)
+    if P == 0:
+        return T, st, g_on, g_cp
+    if L > 1 and (coupling is None or tuple(coupling.shape) != (K, L - 1, n, n)):
+        raise ValueError("rgf_adjoint needs coupling blocks [K, L-1, n, n]")
+    need = int(lib.negf_adjoint_workspace_bytes(n, nl, nr, L))
+    if need == 0:
+        raise RuntimeError(f"block order {max(n, nl, nr)} is not supported by the adjoint kernel")
+    ws = _workspace(need, dev, "adjoint")
+    k_index = k_index.to(device=dev, dtype=torch.int32).contiguous()
+    vl_ks = n * nl if vl.shape[0] > 1 else 0
+    vr_ks = n * nr if vr.shape[0] > 1 else 0
+    cp = coupling if L > 1 else None
+    rc = lib.negf_rgf_adjoint_f64(
+        n, nl, nr, L, P, _lib.ptr(onsite), L * n * n, n * n, _lib.ptr(cp), (L - 1) * n * n, n * n, _lib.ptr(vl),
+        vl_ks, _lib.ptr(vr), vr_ks, _lib.ptr(gl), nl * nl, _lib.ptr(gr), nr * nr, _lib.ptr(k_index),
+        _lib.ptr(omega), _lib.ptr(eta_dev), _lib.ptr(lead_status), _lib.ptr(weight), _lib.ptr(g_on),
+        _lib.ptr(g_cp if L > 1 else None), _lib.ptr(T), _lib.ptr(st), _lib.ptr(ws), ws.numel(),
+        _lib.stream_handle(stream))
+    _lib.check(rc, "negf_rgf_adjoint_f64")
+    return T, st, g_on, g_cp
+
+
 def kavg(T_wk: torch.Tensor, stream=None) -> torch.Tensor:
     """Mean over k of an omega-major ``[W, K]`` table."""
     lib = _lib.load()

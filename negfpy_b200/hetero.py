@@ -1,0 +1,290 @@
+"""Parametric heterojunction device: spring constants -> k-space blocks.
+
+A layered slab of ``ny x nz`` sites per principal layer (3 DOF each, block
+order ``3 ny nz``), periodic in y (one transverse k), with free surfaces in
+z.  Material A (layers ``< n_layers // 2``) occupies the sites with
+z < ``nz_a``; the remaining sites of A layers are inert padding (no springs,
+a stiff onsite pinning, so they carry no phonons in the frequency range, the
+device trick of negfpy's ``tests/test_interface_contacts.py:36-37``).
+Material B (the other layers) occupies every site.  Springs are central
+NN/NNN springs as in ``workloads.spring_network``; A-A, B-B and A-B
+(interface) bonds draw their constants from different ranges, masses per
+material.  Both materials are periodic along x, so the leads are the
+periodic crystals A (order 3 ny nz_a) and B (order 3 ny nz).
+
+The device is described bond by bond.  A set of bonds around the interface
+are parameters: ``theta`` (FP64) overrides their spring constants, and the
+blocks are linear in theta:
+    D(k; theta) = D_fixed(k) + sum_p theta_p dD(k)/dtheta_p.
+``blocks(theta)`` evaluates them on the GPU with torch (differentiable for
+a dense check), ``contract(grad_onsite, grad_coupling)`` turns the adjoint
+blocks of ``negf_rgf_adjoint_f64`` into dkappa/dtheta.
+"""
+
+from __future__ import annotations
+
+from dataclasses import dataclass
+from itertools import product
+
+import numpy as np
+import torch
+
+from .workloads import _half_space_neighbours
+
+
+@dataclass
+class Contrib:
+    """One 3x3 contribution of a bond to a block, per unit spring constant."""
+
+    kind: np.ndarray    # 0 onsite block, 1 coupling block
+    layer: np.ndarray   # block layer
+    row: np.ndarray     # first DOF row
+    col: np.ndarray     # first DOF column
+    phase: np.ndarray   # transverse cell shift multiplying i ky
+    coef: np.ndarray    # [m, 3, 3] real: sign * e e^T / sqrt(m_a m_b)
+    bond: np.ndarray    # bond index
+
+
+class HeteroModel:
+    def __init__(self, seed: int = 4, ny: int = 2, nz_a: int = 8, nz_b: int = 12, n_layers: int = 30,
+                 n_params: int = 2000, pin: float = 100.0):
+        rng = np.random.default_rng(seed)
+        self.ny, self.nz, self.nz_a, self.L = ny, nz_b, nz_a, n_layers
+        self.n_sites = ny * nz_b
+        self.n = 3 * self.n_sites
+        self.n_a = 3 * ny * nz_a
+        self.split = n_layers // 2
+        mass_a = rng.uniform(0.8, 1.2, size=(ny, nz_a))
+        mass_b = rng.uniform(0.9, 1.4, size=(ny, nz_b))
+        # Site tables: device site s = y * nz + z.
+        self.site_y = np.repeat(np.arange(ny), nz_b)
+        self.site_z = np.tile(np.arange(nz_b), ny)
+        self.mass = np.ones((n_layers, self.n_sites))
+        self.active = np.zeros((n_layers, self.n_sites), dtype=bool)
+        for l in range(n_layers):
+            for s in range(self.n_sites):
+                y, z = self.site_y[s], self.site_z[s]
+                if l < self.split:
+                    if z < nz_a:
+                        self.active[l, s] = True
+                        self.mass[l, s] = mass_a[y, z]
+                else:
+                    self.active[l, s] = True
+                    self.mass[l, s] = mass_b[y, z]
+        self.pin = pin
+        # Periodic spring tables per material, keyed by (site, neighbour vector).
+        spr_a = {(s, d): rng.uniform(0.5, 1.5) for s in range(self.n_sites) for d in _half_space_neighbours()}
+        spr_b = {(s, d): rng.uniform(0.8, 1.6) for s in range(self.n_sites) for d in _half_space_neighbours()}
+        spr_i = {(s, d): rng.uniform(0.6, 1.4) for s in range(self.n_sites) for d in _half_space_neighbours()}
+        self._spr = (spr_a, spr_b, spr_i)
+        # Bond instances of the device.  Layers -1 and n_layers stand for the
+        # leads: a spring crossing the device boundary contributes only its
+        # device-side self term (the rest is the lead coupling).
+        la, a, lb, b, cy, ev, k0 = [], [], [], [], [], [], []
+        for s in range(self.n_sites):  # lead A (layer -1) -> device layer 0
+            if self.site_z[s] >= nz_a:
+                continue
+            for d in _half_space_neighbours():
+                dx, dy, dz = d
+                y2, z2 = self.site_y[s] + dy, self.site_z[s] + dz
+                if dx != 1 or z2 < 0 or z2 >= nz_a:
+                    continue
+                c, y2 = divmod(y2, ny)
+                s2 = y2 * nz_b + z2
+                la.append(-1), a.append(s), lb.append(0), b.append(s2), cy.append(c)
+                ev.append(np.asarray(d, float) / np.linalg.norm(d))
+                k0.append(spr_a[(s, d)])
+        for l in range(n_layers):
+            for s in range(self.n_sites):
+                if not self.active[l, s]:
+                    continue
+                for d in _half_space_neighbours():
+                    dx, dy, dz = d
+                    l2 = l + dx
+                    y2, z2 = self.site_y[s] + dy, self.site_z[s] + dz
+                    if z2 < 0 or z2 >= nz_b:
+                        continue
+                    c, y2 = divmod(y2, ny)
+                    s2 = y2 * nz_b + z2
+                    if l2 >= n_layers:  # device layer L-1 -> lead B (layer L)
+                        la.append(l), a.append(s), lb.append(l2), b.append(s2), cy.append(c)
+                        ev.append(np.asarray(d, float) / np.linalg.norm(d))
+                        k0.append(spr_b[(s, d)])
+                        continue
+                    if not self.active[l2, s2]:
+                        continue
+                    ma, mb = l < self.split, l2 < self.split
+                    table = spr_a if (ma and mb) else (spr_b if (not ma and not mb) else spr_i)
+                    la.append(l), a.append(s), lb.append(l2), b.append(s2), cy.append(c)
+                    ev.append(np.asarray(d, float) / np.linalg.norm(d))
+                    k0.append(table[(s, d)])
+        self.bond_la, self.bond_a = np.array(la), np.array(a)
+        self.bond_lb, self.bond_b = np.array(lb), np.array(b)
+        self.bond_cy, self.bond_e, self.bond_k0 = np.array(cy), np.array(ev), np.array(k0)
+        # Parameters: the bonds nearest to the interface layer boundary (never
+        # the half bonds at the device ends).
+        mid = self.split - 0.5
+        dist = np.abs(0.5 * (self.bond_la + self.bond_lb) - mid)
+        dist[(self.bond_la < 0) | (self.bond_lb >= n_layers)] = np.inf
+        order = np.lexsort((np.arange(dist.size), dist))
+        self.param_bonds = np.sort(order[:n_params])
+        self.theta0 = self.bond_k0[self.param_bonds].copy()
+        self.is_param = np.zeros(self.bond_k0.size, dtype=bool)
+        self.is_param[self.param_bonds] = True
+        self.contrib = self._contributions()
+
+    # ---------------------------------------------------------------- blocks
+    def _contributions(self) -> Contrib:
+        kind, layer, row, col, phase, coef, bond = [], [], [], [], [], [], []
+        for i in range(self.bond_k0.size):
+            la, a, lb, b = self.bond_la[i], self.bond_a[i], self.bond_lb[i], self.bond_b[i]
+            e = self.bond_e[i]
+            ee = np.outer(e, e)
+            c = self.bond_cy[i]
+            inside_a, inside_b = 0 <= la < self.L, 0 <= lb < self.L
+            # self terms (device-side ends only)
+            for (inside, l, s) in ((inside_a, la, a), (inside_b, lb, b)):
+                if inside:
+                    kind.append(0), layer.append(l), row.append(3 * s), col.append(3 * s), phase.append(0)
+                    coef.append(ee / self.mass[l, s]), bond.append(i)
+            if not (inside_a and inside_b):
+                continue
+            ma, mb = self.mass[la, a], self.mass[lb, b]
+            w = -ee / np.sqrt(ma * mb)
+            if la == lb:
+                kind += [0, 0]
+                layer += [la, la]
+                row += [3 * a, 3 * b]
+                col += [3 * b, 3 * a]
+                phase += [c, -c]
+                coef += [w, w]
+                bond += [i, i]
+            else:
+                kind.append(1), layer.append(la), row.append(3 * a), col.append(3 * b), phase.append(c)
+                coef.append(w), bond.append(i)
+        return Contrib(np.array(kind), np.array(layer), np.array(row), np.array(col), np.array(phase, float),
+                       np.array(coef), np.array(bond))
+
+    def _pinning(self) -> np.ndarray:
+        on = np.zeros((self.L, self.n, self.n))
+        for l in range(self.L):
+            for s in range(self.n_sites):
+                if not self.active[l, s]:
+                    on[l, 3 * s:3 * s + 3, 3 * s:3 * s + 3] = np.eye(3) * self.pin / self.mass[l, s]
+        return on
+
+    def blocks(self, theta: torch.Tensor, kpoints, device=None):
+        """(onsite [K, L, n, n], coupling [K, L-1, n, n]) complex128 for spring values theta."""
+        dev = device or theta.device
+        ky = torch.as_tensor(np.array([k[0] for k in kpoints], float), device=dev)
+        K, L, n = ky.numel(), self.L, self.n
+        kvals = torch.as_tensor(self.bond_k0, device=dev, dtype=torch.float64).clone()
+        kvals = kvals.index_put((torch.as_tensor(self.param_bonds, device=dev),), theta.to(dev))
+        ct = self.contrib
+        spring = kvals[torch.as_tensor(ct.bond, device=dev)]                      # [m]
+        ph = torch.exp(1j * ky[:, None] * torch.as_tensor(ct.phase, device=dev)[None, :])  # [K, m]
+        val = (spring[None, :, None, None] * ph[:, :, None, None]
+               * torch.as_tensor(ct.coef, device=dev)[None])                        # [K, m, 3, 3]
+        onsite = torch.zeros((K, L * n * n), dtype=torch.complex128, device=dev)
+        coupling = torch.zeros((K, max(L - 1, 1) * n * n), dtype=torch.complex128, device=dev)
+        ar = torch.arange(3, device=dev)
+        r = torch.as_tensor(ct.row, device=dev)[:, None, None] + ar[None, :, None]
+        c = torch.as_tensor(ct.col, device=dev)[:, None, None] + ar[None, None, :]
+        lay = torch.as_tensor(ct.layer, device=dev)[:, None, None]
+        flat = (lay * n * n + r * n + c).expand(-1, 3, 3)                          # [m, 3, 3]
+        kind = torch.as_tensor(ct.kind, device=dev)
+        for kd, tgt in ((0, onsite), (1, coupling)):
+            sel = kind == kd
+            if bool(sel.any()):
+                idx = flat[sel].reshape(-1)
+                tgt.index_add_(1, idx, val[:, sel].reshape(K, -1))
+        onsite = onsite.reshape(K, L, n, n) + torch.as_tensor(self._pinning(), device=dev)[None]
+        return onsite, coupling.reshape(K, max(L - 1, 1), n, n)
+
+    def contract(self, grad_onsite: torch.Tensor, grad_coupling: torch.Tensor, kpoints) -> torch.Tensor:
+        """dkappa/dtheta = 2 Re sum_k Tr[dD/dtheta X] from the accumulated adjoint blocks."""
+        dev = grad_onsite.device
+        ky = torch.as_tensor(np.array([k[0] for k in kpoints], float), device=dev)
+        K, L, n = ky.numel(), self.L, self.n
+        ct = self.contrib
+        sel = torch.as_tensor(self.is_param[ct.bond], device=dev)
+        ar = torch.arange(3, device=dev)
+        # Tr[dD X] = sum_ab dD_ab X_ba: gather X at the transposed positions
+        r = torch.as_tensor(ct.row, device=dev)[:, None, None] + ar[None, :, None]
+        c = torch.as_tensor(ct.col, device=dev)[:, None, None] + ar[None, None, :]
+        lay = torch.as_tensor(ct.layer, device=dev)[:, None, None]
+        flat_t = (lay * n * n + c * n + r)                                         # X[b, a]
+        kind = torch.as_tensor(ct.kind, device=dev)
+        ph = torch.exp(1j * ky[:, None] * torch.as_tensor(ct.phase, device=dev)[None, :])
+        coef = torch.as_tensor(ct.coef, device=dev)
+        out = torch.zeros(self.param_bonds.size, dtype=torch.float64, device=dev)
+        pmap = torch.full((self.bond_k0.size,), -1, dtype=torch.long, device=dev)
+        pmap[torch.as_tensor(self.param_bonds, device=dev)] = torch.arange(self.param_bonds.size, device=dev)
+        for kd, src in ((0, grad_onsite.reshape(K, -1)), (1, grad_coupling.reshape(K, -1))):
+            m = sel & (kind == kd)
+            if not bool(m.any()):
+                continue
+            x = src[:, flat_t[m].reshape(-1)].reshape(K, -1, 3, 3)                # [K, mm, 3, 3]
+            t = (coef[m][None] * x).sum(dim=(2, 3)) * ph[:, m]                    # [K, mm]
+            contrib = 2.0 * t.sum(dim=0).real
+            out.index_add_(0, pmap[torch.as_tensor(ct.bond, device=dev)[m]], contrib)
+        return out
+
+    # ------------------------------------------------------------ the leads
+    def lead_blocks(self, material: str, kpoints) -> dict:
+        """Periodic lead A or B: d00, d01, d10 [K, m, m] with A's sites in its own order."""
+        spr_a, spr_b, _ = self._spr
+        table = spr_a if material == "A" else spr_b
+        nz = self.nz_a if material == "A" else self.nz
+        sites = [(y, z) for y in range(self.ny) for z in range(nz)]
+        index = {s: i for i, s in enumerate(sites)}
+        m = 3 * len(sites)
+        lay = 0 if material == "A" else self.L - 1
+        mass = np.array([self.mass[lay, y * self.nz + z] for y, z in sites])
+        K = len(kpoints)
+        d00 = np.zeros((K, m, m), dtype=complex)
+        d01 = np.zeros((K, m, m), dtype=complex)
+        for ki, kp in enumerate(kpoints):
+            ky = kp[0]
+            for (y, z) in sites:
+                s_dev = y * self.nz + z
+                i = index[(y, z)]
+                for d in _half_space_neighbours():
+                    dx, dy, dz = d
+                    y2, z2 = y + dy, z + dz
+                    if z2 < 0 or z2 >= nz:
+                        continue
+                    c, y2 = divmod(y2, self.ny)
+                    j = index[(y2, z2)]
+                    e = np.asarray(d, float) / np.linalg.norm(d)
+                    ee = table[(s_dev, d)] * np.outer(e, e)
+                    d00[ki, 3 * i:3 * i + 3, 3 * i:3 * i + 3] += ee / mass[i]
+                    d00[ki, 3 * j:3 * j + 3, 3 * j:3 * j + 3] += ee / mass[j]
+                    w = -ee / np.sqrt(mass[i] * mass[j]) * np.exp(1j * ky * c)
+                    if dx == 0:
+                        d00[ki, 3 * i:3 * i + 3, 3 * j:3 * j + 3] += w
+                        d00[ki, 3 * j:3 * j + 3, 3 * i:3 * i + 3] += np.conj(w)
+                    else:
+                        d01[ki, 3 * i:3 * i + 3, 3 * j:3 * j + 3] += w
+        return {"d00": d00, "d01": d01, "d10": np.conj(np.swapaxes(d01, 1, 2)), "sites": sites}
+
+    def omega_max(self, nk: int = 8) -> float:
+        """Largest bulk phonon frequency of the two leads over a (kx, ky) sample."""
+        ks = -np.pi + (np.arange(nk) + 0.5) * (2.0 * np.pi / nk)
+        wmax = 0.0
+        for mat in ("A", "B"):
+            lb = self.lead_blocks(mat, [(k,) for k in ks])
+            for kx in ks:
+                d = lb["d00"] + lb["d01"] * np.exp(1j * kx) + lb["d10"] * np.exp(-1j * kx)
+                d = 0.5 * (d + np.conj(np.swapaxes(d, 1, 2)))
+                wmax = max(wmax, float(np.sqrt(max(np.linalg.eigvalsh(d).max(), 0.0))))
+        return wmax
+
+    def contact_left_indices(self) -> np.ndarray:
+        """Device DOFs of layer 0 in lead A's DOF order."""
+        idx = []
+        for y in range(self.ny):
+            for z in range(self.nz_a):
+                s = y * self.nz + z
+                idx += [3 * s, 3 * s + 1, 3 * s + 2]
+        return np.array(idx)

@@ -1,0 +1,74 @@
+"""Host checks of the heterojunction model (no GPU): the device blocks of the
+A and B regions reproduce the periodic leads, the blocks are Hermitian, the
+leads are positive semidefinite and the contraction is the exact derivative
+of a linear functional of the blocks."""
+
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from negfpy_b200.adjoint import kappa_weights
+from negfpy_b200.hetero import HeteroModel
+
+KP = [(-2.2,), (0.4,)]
+
+
+def _blocks(m, theta=None):
+    th = torch.as_tensor(m.theta0 if theta is None else theta, dtype=torch.float64)
+    on, cp = m.blocks(th, KP)
+    return on.numpy(), cp.numpy()
+
+
+def test_sizes_of_the_differentiation_configuration():
+    m = HeteroModel()
+    assert (m.n_a, m.n, m.L, m.theta0.size) == (48, 72, 30, 2000)
+    assert set(m.bond_la[m.param_bonds]) | set(m.bond_lb[m.param_bonds]) <= set(range(1, m.L - 1))
+
+
+def test_regions_reproduce_the_leads():
+    m = HeteroModel(seed=1, ny=2, nz_a=2, nz_b=3, n_layers=8, n_params=30)
+    on, cp = _blocks(m)
+    la, lb = m.lead_blocks("A", KP), m.lead_blocks("B", KP)
+    ia = m.contact_left_indices()
+    for l in range(1, m.split - 1):
+        np.testing.assert_allclose(on[:, l][:, ia[:, None], ia], la["d00"], atol=1e-13)
+        np.testing.assert_allclose(cp[:, l][:, ia[:, None], ia], la["d01"], atol=1e-13)
+    np.testing.assert_allclose(on[:, 0][:, ia[:, None], ia], la["d00"], atol=1e-13)
+    for l in range(m.split + 1, m.L):
+        np.testing.assert_allclose(on[:, l], lb["d00"], atol=1e-13)
+    np.testing.assert_allclose(cp[:, m.L - 2], lb["d01"], atol=1e-13)
+
+
+def test_hermitian_and_psd():
+    m = HeteroModel(seed=2, ny=2, nz_a=2, nz_b=3, n_layers=6, n_params=20)
+    on, _ = _blocks(m)
+    assert np.abs(on - np.conj(np.swapaxes(on, -1, -2))).max() < 1e-14
+    for mat in ("A", "B"):
+        lb = m.lead_blocks(mat, [(0.0,)])
+        d = lb["d00"][0] + lb["d01"][0] + lb["d10"][0]  # kx = 0 bulk matrix
+        assert np.linalg.eigvalsh(d).min() > -1e-12
+
+
+def test_contract_is_the_derivative_of_a_linear_functional():
+    """For F(theta) = 2 Re sum Tr[D(theta) X] with fixed X, contract(X) = dF/dtheta."""
+    m = HeteroModel(seed=3, ny=2, nz_a=2, nz_b=3, n_layers=6, n_params=25)
+    rng = np.random.default_rng(0)
+    K, L, n = len(KP), m.L, m.n
+    xo = torch.as_tensor(rng.normal(size=(K, L, n, n)) + 1j * rng.normal(size=(K, L, n, n)))
+    xc = torch.as_tensor(rng.normal(size=(K, L - 1, n, n)) + 1j * rng.normal(size=(K, L - 1, n, n)))
+    th = torch.as_tensor(m.theta0, dtype=torch.float64).clone().requires_grad_(True)
+    on, cp = m.blocks(th, KP)
+    f = 2 * (torch.einsum("klab,klba->", on, xo) + torch.einsum("klab,klba->", cp, xc)).real
+    (g_ref,) = torch.autograd.grad(f, th)
+    g = m.contract(xo, xc, KP)
+    np.testing.assert_allclose(g.numpy(), g_ref.numpy(), rtol=1e-12, atol=1e-12 * float(g_ref.abs().max()))
+
+
+def test_kappa_weights_trapezoid():
+    om = torch.linspace(0.01, 3.0, 301, dtype=torch.float64)
+    w = kappa_weights(om, 300.0, 1e13)
+    # constant T = 1 integrates the Bose kernel; compare with a fine midpoint sum
+    fine = torch.linspace(0.01, 3.0, 300001, dtype=torch.float64)
+    wf = kappa_weights(fine, 300.0, 1e13)
+    assert abs(float(w.sum() / wf.sum()) - 1) < 1e-4
