@@ -46,6 +46,8 @@ def _args():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--omegas", type=int, default=N_OMEGA,
                     help="omegas per rank (default: the full 2048; smaller values are profiling cases)")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the refined-precision and gradient measurements (run at N=1 only)")
     ap.add_argument("--kernels-only", action="store_true",
                     help="time the kernels only (no e2e, CPU baseline or peak probe); for profiling runs")
     return ap.parse_args()
@@ -172,6 +174,82 @@ def fp64_peak_tflops(torch):
     del a, b
     torch.cuda.empty_cache()
     return 2.0 * 8192 ** 3 / best / 1e12
+
+
+def refined_vs_f64(torch, omega_stride=16):
+    """Refined (FP64 surface GF + mixed-precision device solve with FP64
+    fallback) against plain FP64 on the 3D bulk workload: n = 96, 16 x 16 k,
+    40 identical layers, every ``omega_stride``-th of 4096 omegas.  Both paths
+    run the same points; kappa(300 K) on that grid is compared."""
+    from negfpy_b200 import engine, spectrum, workloads as Wm
+    from negfpy_b200.adjoint import kappa_weights
+
+    wl = Wm.bulk_workload()
+    s = engine.StackedSystem.from_arrays(wl.lead_l, wl.lead_l, wl.onsite, wl.coupling, wl.n_layers)
+    wi = np.arange(0, wl.omegas.size, omega_stride)
+    K = len(wl.kpoints)
+    om_w = torch.tensor(wl.omegas[wi], dtype=torch.float64, device="cuda")
+    w_idx, k_idx = spectrum.grid_points(len(wi), K, om_w.device)
+    om = om_w[w_idx].contiguous()
+    eta = torch.full_like(om, wl.eta)
+    warm = slice(0, 4 * K)
+    for prec in ("f64", "refined"):
+        s.transmission(om[warm], k_idx[warm], eta[warm], precision=prec)
+    res, ms = {}, {}
+    for prec in ("f64", "refined"):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        res[prec] = s.transmission(om, k_idx, eta, precision=prec)
+        e1.record()
+        torch.cuda.synchronize()
+        ms[prec] = e0.elapsed_time(e1)
+    P = int(om.numel())
+    w = kappa_weights(om_w, 300.0, wl.omega_unit_rad_s)
+    kap = {p: float((w * res[p]["T"].reshape(len(wi), K).mean(1)).sum()) for p in res}
+    t64, tr = res["f64"]["T"], res["refined"]["T"]
+    return {"workload": f"bulk_n96_L40_K256, every {omega_stride}th of 4096 omegas ({P} points)",
+            "f64_points_per_s": P / ms["f64"] * 1e3, "refined_points_per_s": P / ms["refined"] * 1e3,
+            "speedup": ms["f64"] / ms["refined"], "kappa_rel_err": (kap["refined"] - kap["f64"]) / kap["f64"],
+            "T_max_rel_err": float(((tr - t64).abs() / t64.abs().clamp_min(1.0)).max()),
+            "fallback_points": int(res["refined"]["fallback"]),
+            "method": "FP64 Sancho-Rubio; device sweep FP32 on 3xTF32 mma.sync with FP64 Sigma/Gamma/trace; "
+                      "FP64 re-solve of failed points"}
+
+
+def grad_vs_forward(torch, n_k=8, n_omega=256, reps=3):
+    """dkappa/dtheta through the adjoint kernel against the forward device solve
+    on the heterojunction (lead 48 | 30 layers of order 72 | lead 72, 2000
+    spring parameters): ratio of CUDA-event times."""
+    from negfpy_b200 import adjoint
+
+    e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    e[0].record()
+    pr = adjoint.hetero_problem(n_k=n_k, n_omega=n_omega)  # lead surface GFs (once per problem)
+    e[1].record()
+    torch.cuda.synchronize()
+    theta = torch.as_tensor(pr.model.theta0, device="cuda")
+    pr.kappa_of_t(pr.transmission(theta))
+    pr.kappa_and_grad(theta)
+    torch.cuda.synchronize()
+    e[2].record()
+    for _ in range(reps):
+        pr.kappa_of_t(pr.transmission(theta))
+    e[3].record()
+    torch.cuda.synchronize()
+    fwd = e[2].elapsed_time(e[3]) / reps
+    g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    g0.record()
+    for _ in range(reps):
+        pr.kappa_and_grad(theta)
+    g1.record()
+    torch.cuda.synchronize()
+    grad = g0.elapsed_time(g1) / reps
+    return {"workload": f"heterojunction lead48|L30 n72|lead72, 2000 params, {n_omega} omega x {n_k} k",
+            "forward_ms": fwd, "grad_ms": grad, "grad_over_forward": grad / fwd,
+            "lead_sgf_ms_once": e[0].elapsed_time(e[1]),
+            "note": "forward = theta -> blocks -> device solve -> kappa; grad = the adjoint kernel (forward "
+                    "sweeps recomputed inside) + contraction to theta; lead GFs do not depend on theta"}
 
 
 def run_reference(args):
@@ -343,6 +421,11 @@ def main():
                "sample": f"{nsamp} random points of the {W}x{K} grid ({dt:.1f} s wall); negfpy's algorithm "
                          "restated in oracle/ (numpy inv + SuperLU), spawn pool, 1 BLAS thread per process"}
 
+    extras = {}
+    if ws == 1 and not args.no_extras:
+        extras["refined"] = refined_vs_f64(torch)
+        extras["grad"] = grad_vs_forward(torch)
+
     if rank == 0:
         out = {
             "metric": METRIC, "value": value, "unit": "points/s", "n_gpus": ws, "steps": args.steps,
@@ -358,6 +441,7 @@ def main():
             "status_ok_fraction": float(np.mean(status == 0)),
             "clocks": clk.summary(),
         }
+        out.update(extras)
         print(json.dumps(out), flush=True)
     if ws > 1:
         dist.barrier()

@@ -127,6 +127,29 @@ int negf_rgf_transmission_f64_noalloc(int n_dev, int n_lead_l, int n_lead_r, int
                                       const int* k_index, const double* omega, const double* eta_device,
                                       const int* lead_status, double* t_out, int* status_out, void* stream);
 
+/* Workspace bytes negf_rgf_transmission_mixed needs (0 on a bad size). */
+size_t negf_rgf_mixed_workspace_bytes(int n_dev, int n_lead_l, int n_lead_r);
+
+/*
+ * Batched device solve and transmission in mixed precision: the same
+ * arguments, outputs and status codes as negf_rgf_transmission_f64 (the
+ * negfpy routines it replaces are those of core/negf.py:72-357).  The contact
+ * self-energies, the broadenings and the trace are FP64; the recursive sweep
+ * through the layers runs in FP32 (3 x TF32 tensor-core products, FP32
+ * Gauss-Jordan).  A point whose FP32 sweep meets a singular or non-finite
+ * pivot reports NEGF_SINGULAR / NEGF_NONFINITE so that the caller can
+ * re-solve it with negf_rgf_transmission_f64.  Block orders 1..256.
+ */
+int negf_rgf_transmission_mixed(int n_dev, int n_lead_l, int n_lead_r, int n_layers, int batch,
+                                const double* onsite, long long onsite_kstride, long long onsite_lstride,
+                                const double* coupling, long long coupling_kstride, long long coupling_lstride,
+                                const double* v_left, long long v_left_kstride, const double* v_right,
+                                long long v_right_kstride, const double* g_left, long long g_left_pstride,
+                                const double* g_right, long long g_right_pstride, const int* k_index,
+                                const double* omega, const double* eta_device, const int* lead_status,
+                                double* t_out, int* status_out, void* workspace, size_t workspace_bytes,
+                                void* stream);
+
 /* Workspace bytes negf_rgf_adjoint_f64 needs (0 on a bad size). */
 size_t negf_adjoint_workspace_bytes(int n_dev, int n_lead_l, int n_lead_r, int n_layers);
 

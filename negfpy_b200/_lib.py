@@ -43,6 +43,12 @@ _SIGNATURES = {
         [_I, _I, _I, _I, _I, _P, _LL, _LL, _P, _LL, _LL, _P, _LL, _P, _LL, _P, _LL, _P, _LL, _P, _P, _P, _P, _P,
          _P, _P],
     ),
+    "negf_rgf_mixed_workspace_bytes": (_SZ, [_I, _I, _I]),
+    "negf_rgf_transmission_mixed": (
+        _I,
+        [_I, _I, _I, _I, _I, _P, _LL, _LL, _P, _LL, _LL, _P, _LL, _P, _LL, _P, _LL, _P, _LL, _P, _P, _P, _P, _P,
+         _P, _P, _SZ, _P],
+    ),
     "negf_adjoint_workspace_bytes": (_SZ, [_I, _I, _I, _I]),
     "negf_rgf_adjoint_f64": (
         _I,

@@ -173,6 +173,75 @@ int negf_rgf_transmission_f64(int n_dev, int n_lead_l, int n_lead_r, int n_layer
   return 0;
 }
 
+size_t negf_rgf_mixed_workspace_bytes(int n_dev, int n_lead_l, int n_lead_r) {
+  if (n_dev <= 0 || n_lead_l <= 0 || n_lead_r <= 0) return 0;
+  const int np = negf::mixed_order(max3(n_dev, n_lead_l, n_lead_r));
+  if (np == 0) return 0;
+  const int grid = negf::rgf_mixed_grid(np);
+  if (grid <= 0) return 0;
+  return kCounterBytes + negf::rgf_mixed_ws_bytes(np, n_dev, grid);
+}
+
+int negf_rgf_transmission_mixed(int n_dev, int n_lead_l, int n_lead_r, int n_layers, int batch,
+                                const double* onsite, long long onsite_kstride, long long onsite_lstride,
+                                const double* coupling, long long coupling_kstride, long long coupling_lstride,
+                                const double* v_left, long long v_left_kstride, const double* v_right,
+                                long long v_right_kstride, const double* g_left, long long g_left_pstride,
+                                const double* g_right, long long g_right_pstride, const int* k_index,
+                                const double* omega, const double* eta_device, const int* lead_status,
+                                double* t_out, int* status_out, void* workspace, size_t workspace_bytes,
+                                void* stream) {
+  if (n_dev <= 0 || n_lead_l <= 0 || n_lead_r <= 0 || n_layers <= 0 || batch < 0)
+    return fail(NEGF_EINVAL, "negf_rgf_transmission_mixed: sizes must be positive");
+  if (!onsite || !v_left || !v_right || !g_left || !g_right || !omega || !eta_device || !t_out)
+    return fail(NEGF_EINVAL, "negf_rgf_transmission_mixed: null pointer");
+  if (n_layers > 1 && !coupling) return fail(NEGF_EINVAL, "negf_rgf_transmission_mixed: null coupling");
+  if (onsite_kstride < 0 || onsite_lstride < 0 || coupling_kstride < 0 || coupling_lstride < 0 ||
+      v_left_kstride < 0 || v_right_kstride < 0 || g_left_pstride < 0 || g_right_pstride < 0)
+    return fail(NEGF_EINVAL, "negf_rgf_transmission_mixed: negative stride");
+  const int np = negf::mixed_order(max3(n_dev, n_lead_l, n_lead_r));
+  if (np == 0) return fail(NEGF_EUNSUPPORTED, "negf_rgf_transmission_mixed: block order above 256");
+  const int grid = negf::rgf_mixed_grid(np);
+  if (grid <= 0) return cuda_fail("negf_rgf_transmission_mixed: occupancy query");
+  if (!workspace || workspace_bytes < kCounterBytes + negf::rgf_mixed_ws_bytes(np, n_dev, grid))
+    return fail(NEGF_EINVAL, "negf_rgf_transmission_mixed: workspace missing or too small");
+  if (batch == 0) return 0;
+  negf::RgfArgs a;
+  a.n = n_dev;
+  a.nl = n_lead_l;
+  a.nr = n_lead_r;
+  a.L = n_layers;
+  a.batch = batch;
+  a.D = reinterpret_cast<const double2*>(onsite);
+  a.d_ks = onsite_kstride;
+  a.d_ls = onsite_lstride;
+  a.C = reinterpret_cast<const double2*>(coupling ? coupling : onsite);
+  a.c_ks = coupling_kstride;
+  a.c_ls = coupling_lstride;
+  a.VL = reinterpret_cast<const double2*>(v_left);
+  a.vl_ks = v_left_kstride;
+  a.VR = reinterpret_cast<const double2*>(v_right);
+  a.vr_ks = v_right_kstride;
+  a.gL = reinterpret_cast<const double2*>(g_left);
+  a.gl_ps = g_left_pstride;
+  a.gR = reinterpret_cast<const double2*>(g_right);
+  a.gr_ps = g_right_pstride;
+  a.kidx = k_index;
+  a.omega = omega;
+  a.eta_dev = eta_device;
+  a.lead_status = lead_status;
+  a.T_out = t_out;
+  a.status_out = status_out;
+  a.counter = reinterpret_cast<unsigned int*>(workspace);
+  a.sigma_ws = nullptr;
+  cudaStream_t st = as_stream(stream);
+  if (cudaMemsetAsync(workspace, 0, sizeof(unsigned int), st) != cudaSuccess)
+    return cuda_fail("negf_rgf_transmission_mixed: counter reset");
+  if (negf::rgf_mixed_launch(a, np, grid, static_cast<char*>(workspace) + kCounterBytes, st) != 0)
+    return cuda_fail("negf_rgf_transmission_mixed");
+  return 0;
+}
+
 size_t negf_adjoint_workspace_bytes(int n_dev, int n_lead_l, int n_lead_r, int n_layers) {
   if (n_dev <= 0 || n_lead_l <= 0 || n_lead_r <= 0 || n_layers <= 0) return 0;
   const int nmax = max3(n_dev, n_lead_l, n_lead_r);

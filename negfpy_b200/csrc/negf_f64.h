@@ -66,6 +66,12 @@ size_t rgf_global_ws_bytes(int np, int n, int grid);
 int sr_f64_global_launch(const SrArgs& a, int np, int grid, double2* ws, unsigned* counter, cudaStream_t st);
 int rgf_f64_global_launch(const RgfArgs& a, int np, int grid, double2* ws, cudaStream_t st);
 
+// Mixed precision device solve (FP32 sweep, FP64 self-energies and trace), orders 1..256.
+int mixed_order(int n);  // padded order (multiple of 16), 0 if unsupported
+int rgf_mixed_grid(int np);
+size_t rgf_mixed_ws_bytes(int np, int n, int grid);
+int rgf_mixed_launch(const RgfArgs& a, int np, int grid, void* ws, cudaStream_t st);
+
 size_t grad_ws_bytes(int np, int n, int L, int grid);
 int grad_grid(int np);
 int grad_f64_launch(const GradArgs& ga, int np, int grid, double2* ws, cudaStream_t st);

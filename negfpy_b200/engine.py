@@ -87,9 +87,15 @@ def _workspace(nbytes: int, dev: torch.device, role: str = "rgf") -> torch.Tenso
 def rgf_transmission(onsite: torch.Tensor, coupling: torch.Tensor | None, n_layers: int, vl: torch.Tensor,
                      vr: torch.Tensor, gl: torch.Tensor, gr: torch.Tensor, omega: torch.Tensor,
                      eta_dev: torch.Tensor, k_index: torch.Tensor | None, lead_status: torch.Tensor | None,
-                     stream=None) -> tuple[torch.Tensor, torch.Tensor]:
+                     stream=None, precision: str = "f64") -> tuple[torch.Tensor, torch.Tensor]:
     """T for P points.  ``onsite`` ``[K, L|1, n, n]``, ``coupling`` ``[K, L-1|1, n, n]``,
-    ``vl`` ``[K|1, n, nl]``, ``vr`` ``[K|1, n, nr]``, ``gl`` ``[P, nl, nl]``, ``gr`` ``[P, nr, nr]``."""
+    ``vl`` ``[K|1, n, nl]``, ``vr`` ``[K|1, n, nr]``, ``gl`` ``[P, nl, nl]``, ``gr`` ``[P, nr, nr]``.
+
+    ``precision``: "f64" (``negf_rgf_transmission_f64``) or "mixed"
+    (``negf_rgf_transmission_mixed``: FP32 sweep, FP64 self-energies and trace;
+    no fallback here, failed points keep their status)."""
+    if precision not in ("f64", "mixed"):
+        raise ValueError(f"unknown precision {precision!r}; expected 'f64' or 'mixed'")
     lib = _lib.load()
     dev = _dev()
     K, Lo, n, _ = onsite.shape
@@ -108,19 +114,42 @@ def rgf_transmission(onsite: torch.Tensor, coupling: torch.Tensor | None, n_laye
         cp, cp_ks, cp_ls = coupling, (Lc * n * n if Kc > 1 else 0), (0 if Lc == 1 else n * n)
     vl_ks = n * nl if vl.shape[0] > 1 else 0
     vr_ks = n * nr if vr.shape[0] > 1 else 0
-    need = int(lib.negf_rgf_workspace_bytes(n, nl, nr))
+    mixed = precision == "mixed"
+    need = int(lib.negf_rgf_mixed_workspace_bytes(n, nl, nr) if mixed else lib.negf_rgf_workspace_bytes(n, nl, nr))
     if need == 0:
-        raise RuntimeError(f"block order {max(n, nl, nr)} is not supported by the FP64 kernels")
-    ws = _workspace(need, dev)
+        raise RuntimeError(f"block order {max(n, nl, nr)} is not supported by the {precision} kernels")
+    ws = _workspace(need, dev, "rgf_mixed" if mixed else "rgf")
     if k_index is not None:
         k_index = k_index.to(device=dev, dtype=torch.int32).contiguous()
-    rc = lib.negf_rgf_transmission_f64(
+    fn = lib.negf_rgf_transmission_mixed if mixed else lib.negf_rgf_transmission_f64
+    rc = fn(
         n, nl, nr, int(n_layers), P, _lib.ptr(onsite), on_ks, on_ls, _lib.ptr(cp), cp_ks, cp_ls, _lib.ptr(vl), vl_ks,
         _lib.ptr(vr), vr_ks, _lib.ptr(gl), nl * nl, _lib.ptr(gr), nr * nr, _lib.ptr(k_index), _lib.ptr(omega),
         _lib.ptr(eta_dev), _lib.ptr(lead_status), _lib.ptr(T), _lib.ptr(st), _lib.ptr(ws), ws.numel(),
         _lib.stream_handle(stream))
-    _lib.check(rc, "negf_rgf_transmission_f64")
+    _lib.check(rc, "negf_rgf_transmission_mixed" if mixed else "negf_rgf_transmission_f64")
     return T, st
+
+
+def rgf_transmission_refined(onsite, coupling, n_layers, vl, vr, gl, gr, omega, eta_dev, k_index, lead_status,
+                             stream=None) -> tuple[torch.Tensor, torch.Tensor, int]:
+    """Mixed-precision device solve with an FP64 fallback: points whose FP32
+    sweep failed (singular or non-finite pivot) while their leads succeeded are
+    solved again by the FP64 kernel.  Returns (T, status, number re-solved)."""
+    T, st = rgf_transmission(onsite, coupling, n_layers, vl, vr, gl, gr, omega, eta_dev, k_index, lead_status,
+                             stream, precision="mixed")
+    bad = st != 0
+    if lead_status is not None:
+        bad &= lead_status == 0
+    idx = torch.nonzero(bad).flatten()
+    nbad = int(idx.numel())
+    if nbad:
+        ki = None if k_index is None else k_index[idx]
+        t2, s2 = rgf_transmission(onsite, coupling, n_layers, vl, vr, gl[idx].contiguous(), gr[idx].contiguous(),
+                                  omega[idx].contiguous(), eta_dev[idx].contiguous(), ki, None, stream)
+        T[idx] = t2
+        st[idx] = s2
+    return T, st, nbad
 
 
 def rgf_adjoint(onsite: torch.Tensor, coupling: torch.Tensor, n_layers: int, vl: torch.Tensor, vr: torch.Tensor,
@@ -243,8 +272,15 @@ class StackedSystem:
 
     def transmission(self, omega: torch.Tensor, k_index: torch.Tensor, eta: torch.Tensor,
                      eta_dev: torch.Tensor | None = None, tol: float = 1e-12, maxiter: int = 200,
-                     chunk: int = 1 << 15, stream=None) -> dict:
-        """T, status and decimation counts for P points (float64/int32 tensors)."""
+                     chunk: int = 1 << 15, stream=None, precision: str = "f64") -> dict:
+        """T, status and decimation counts for P points (float64/int32 tensors).
+
+        ``precision="refined"``: FP64 surface GFs, mixed-precision device solve
+        with the FP64 fallback of ``rgf_transmission_refined``; the result also
+        carries ``fallback`` (points re-solved in FP64)."""
+        if precision not in ("f64", "refined"):
+            raise ValueError(f"unknown precision {precision!r}; expected 'f64' or 'refined'")
+        n_fallback = 0
         dev = _dev()
         P = int(omega.shape[0])
         omega = _r(omega, dev)
@@ -266,10 +302,15 @@ class StackedSystem:
             else:
                 rr = sgf_sr(*self.lead_r, om, et, ki, tol, maxiter, stream=stream)
                 lst = torch.where(rl["status"] != 0, rl["status"], rr["status"])
-            t, s = rgf_transmission(self.onsite, self.coupling, self.n_layers, self.vl, self.vr, rl["g"], rr["g"],
-                                    om, ed, ki, lst, stream=stream)
+            if precision == "refined":
+                t, s, nb = rgf_transmission_refined(self.onsite, self.coupling, self.n_layers, self.vl, self.vr,
+                                                    rl["g"], rr["g"], om, ed, ki, lst, stream=stream)
+                n_fallback += nb
+            else:
+                t, s = rgf_transmission(self.onsite, self.coupling, self.n_layers, self.vl, self.vr, rl["g"],
+                                        rr["g"], om, ed, ki, lst, stream=stream)
             T[sl] = t
             st[sl] = s
             itl[sl] = rl["iters"]
             itr[sl] = rr["iters"]
-        return {"T": T, "status": st, "iters_left": itl, "iters_right": itr}
+        return {"T": T, "status": st, "iters_left": itl, "iters_right": itr, "fallback": n_fallback}

@@ -59,7 +59,7 @@ def transmission_grid(omegas, kpoints, device, lead_left, lead_right, eta: float
     P = om.size * K
     r = sysobj.transmission(om_t, k_idx, torch.full((P,), eta / s, dtype=torch.float64, device=dev),
                             torch.full((P,), eta_dev / s, dtype=torch.float64, device=dev), tol, maxiter)
-    return {key: v.reshape(om.size, K).cpu().numpy() for key, v in r.items()}
+    return {key: v.reshape(om.size, K).cpu().numpy() for key, v in r.items() if torch.is_tensor(v)}
 
 
 def kappa_from_grid(omegas, T_wk, temperatures, omega_unit_rad_s: float) -> np.ndarray:
