@@ -252,6 +252,77 @@ def grad_vs_forward(torch, n_k=8, n_omega=256, reps=3):
                     "sweeps recomputed inside) + contraction to theta; lead GFs do not depend on theta"}
 
 
+def uneven_batch(torch, omega_stride=256):
+    """The uneven batch (64 seeded systems, n in {24..192}, 10-60 layers,
+    1-256 k, 1024 omegas each) on every ``omega_stride``-th omega of each
+    system: autotuned launch shape and item order, one persistent launch per
+    solve replayed from a CUDA graph, FP64 and refined (mixed device sweep with
+    FP64 re-solve of failed items).  Reports points/s of both and the
+    per-system kappa(300 K) error of the refined result against FP64."""
+    from negfpy_b200 import workloads as Wm
+    from negfpy_b200.adjoint import kappa_weights
+    from negfpy_b200.autotune import BatchTuner
+    from negfpy_b200.batch import UnevenBatch
+
+    ws = Wm.uneven_workload()
+    b = UnevenBatch(ws)
+    oms = [w.omegas[omega_stride // 2::omega_stride] for w in ws]
+    tune_oms = [w.omegas[512:513] for w in ws]
+    import tempfile
+
+    tuner = BatchTuner(Path(tempfile.gettempdir()) / "negfpy_b200_bench_tune.json")
+    out, res = {}, {}
+    for prec in ("f64", "mixed"):
+        c = tuner.tune(b, prec, tune_oms, reps=1, force=True)
+        it = b.items(oms, c["order"])
+        g, (T, st, _) = b.graph(it, prec, blocks_per_sm=c["blocks_per_sm"])
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        g.replay()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        bad = st != 0
+        nfb = int(((st == 2) | (st == 3)).sum()) if prec == "mixed" else 0
+        if nfb:
+            idx = torch.nonzero((st == 2) | (st == 3)).flatten()
+            from negfpy_b200.batch import Items
+            sub = Items(it.system[idx].contiguous(), it.k[idx].contiguous(), it.omega[idx].contiguous(), idx,
+                        it.cost[idx.cpu().numpy()])
+            e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e2.record()
+            t2, s2, _ = b.launch(sub, "f64")
+            e3.record()
+            torch.cuda.synchronize()
+            ms += e2.elapsed_time(e3)
+            T[idx], st[idx] = t2, s2
+        Tc = torch.empty_like(T)
+        Tc[it.perm] = T
+        res[prec] = Tc
+        P = int(it.system.numel())
+        out[prec] = {"points_per_s": P / ms * 1e3, "ms": ms, "blocks_per_sm": c["blocks_per_sm"],
+                     "order": c["order"], "failed": int(bad.sum()), "fallback": nfb,
+                     "tuning_ms": {k: round(v, 1) for k, v in c["timings"].items()}}
+        del g
+    offs = np.cumsum([0] + [o.size * len(w.kpoints) for o, w in zip(oms, ws)])
+    errs = []
+    for i, w in enumerate(ws):
+        K = len(w.kpoints)
+        wk = kappa_weights(torch.as_tensor(oms[i], device="cuda"), 300.0, w.omega_unit_rad_s)
+        a = res["f64"][offs[i]:offs[i + 1]].reshape(-1, K).mean(1)
+        m = res["mixed"][offs[i]:offs[i + 1]].reshape(-1, K).mean(1)
+        k64 = float((wk * a).sum())
+        errs.append((float((wk * m).sum()) - k64) / k64)
+    errs = np.abs(np.array(errs))
+    return {"workload": f"64 systems, n in {{24..192}}, L 10-60, K 1-256, every {omega_stride}th of 1024 omegas "
+                        f"({int(offs[-1])} points)",
+            "f64": out["f64"], "refined": out["mixed"],
+            "speedup": out["mixed"]["points_per_s"] / out["f64"]["points_per_s"],
+            "kappa_rel_err_max": float(errs.max()), "kappa_rel_err_median": float(np.median(errs)),
+            "launch": "one persistent kernel per solve, replayed from a CUDA graph; shape and order autotuned"}
+
+
 def run_reference(args):
     ws, rank, _ = _dist()
     if rank != 0:
@@ -425,6 +496,7 @@ def main():
     if ws == 1 and not args.no_extras:
         extras["refined"] = refined_vs_f64(torch)
         extras["grad"] = grad_vs_forward(torch)
+        extras["uneven_batch"] = uneven_batch(torch)
 
     if rank == 0:
         out = {

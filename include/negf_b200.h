@@ -34,6 +34,7 @@ extern "C" {
 #define NEGF_NONFINITE 2
 #define NEGF_SINGULAR 3
 #define NEGF_REFINE_FAIL 4
+#define NEGF_BAD_ITEM 5 /* batch item: system, k index or block order out of range */
 
 #define NEGF_EINVAL (-1)
 #define NEGF_EUNSUPPORTED (-2)
@@ -175,6 +176,71 @@ int negf_rgf_adjoint_f64(int n_dev, int n_lead_l, int n_lead_r, int n_layers, in
                          const double* eta_device, const int* lead_status, const double* weight, double* grad_onsite,
                          double* grad_coupling, double* t_out, int* status_out, void* workspace,
                          size_t workspace_bytes, void* stream);
+
+/*
+ * One lead/device/lead system of an uneven batch (negf_batch_transmission).
+ * Pointers are device pointers to complex128 (interleaved re, im) blocks with
+ * the layouts of negf_sgf_sr_f64 and negf_rgf_transmission_f64: lead set k at
+ * lead_*_h00/h01/h10 + k*lead_*_kstride (h10 NULL: h01^H), onsite block (k, l)
+ * at onsite + k*onsite_kstride + l*onsite_lstride, and so on.  same_leads
+ * nonzero: the right lead is the left one (one decimation per item; then
+ * n_lead_r must equal n_lead_l).  n_k: number of k sets; items with k outside
+ * [0, n_k) report NEGF_BAD_ITEM.
+ */
+typedef struct NegfBatchSystem {
+  int n_dev, n_lead_l, n_lead_r, n_layers, n_k, same_leads;
+  const double* onsite;
+  long long onsite_kstride, onsite_lstride;
+  const double* coupling;
+  long long coupling_kstride, coupling_lstride;
+  const double* v_left;
+  long long v_left_kstride;
+  const double* v_right;
+  long long v_right_kstride;
+  const double* lead_l_h00;
+  const double* lead_l_h01;
+  const double* lead_l_h10;
+  long long lead_l_kstride;
+  const double* lead_r_h00;
+  const double* lead_r_h01;
+  const double* lead_r_h10;
+  long long lead_r_kstride;
+  double eta, eta_device;
+} NegfBatchSystem;
+
+/* Largest persistent grid (blocks) of the batch kernel for systems of block
+ * order up to max_order; precision 0 = FP64 device solve, 1 = mixed;
+ * blocks_per_sm 1 or 2 selects the kernel variant whose registers are capped
+ * for that many resident blocks (0 on a bad argument). */
+int negf_batch_max_grid(int max_order, int precision, int blocks_per_sm);
+
+/* Workspace bytes of negf_batch_transmission (grid <= 0: the largest grid). */
+size_t negf_batch_workspace_bytes(int max_order, int precision, int blocks_per_sm, int grid);
+
+/* sizeof(NegfBatchSystem), for bindings that lay the table out themselves. */
+size_t negf_batch_system_bytes(void);
+
+/*
+ * Uneven batch in one persistent launch: item i is system item_system[i] of
+ * the device-memory table `systems` at its k set item_k[i] and frequency
+ * item_omega[i].  Per item: the lead decimation(s) of negf_sgf_sr_f64 and the
+ * device solve of negf_rgf_transmission_f64 (precision 0) or of
+ * negf_rgf_transmission_mixed (precision 1), i.e. negfpy core/negf.py:306-357
+ * per (system, omega, k).  Items run in the given order, one block each, taken
+ * from a work counter: order them by decreasing cost for a short tail.
+ * Outputs per item: t_out (NaN on failure), status_out (NEGF_* codes,
+ * NEGF_BAD_ITEM for an out-of-range system index, k index or block order
+ * above max_order), iters_out (left lead's decimation sweeps); the last two
+ * may be NULL.  blocks_per_sm: kernel variant (1 or 2, see
+ * negf_batch_max_grid); grid: blocks (<= negf_batch_max_grid; <= 0 picks it).  The
+ * launch (a counter reset and one kernel) can be captured in a CUDA graph once
+ * a call with the same max_order and precision has run outside the capture.
+ */
+int negf_batch_transmission(const NegfBatchSystem* systems, int n_systems, int max_order, const int* item_system,
+                            const int* item_k, const double* item_omega, int n_items, double tol, int maxiter,
+                            int precision, int blocks_per_sm, int grid, double* t_out, int* status_out,
+                            int* iters_out,
+                            void* workspace, size_t workspace_bytes, void* stream);
 
 /*
  * k average of an omega-major [n_omega][n_k] transmission table.

@@ -17,8 +17,9 @@ from . import _build
 _lock = threading.Lock()
 _lib = None
 
-OK, MAXITER, NONFINITE, SINGULAR, REFINE_FAIL = 0, 1, 2, 3, 4
-STATUS_NAMES = {OK: "ok", MAXITER: "maxiter", NONFINITE: "non_finite", SINGULAR: "singular", REFINE_FAIL: "refine_failed"}
+OK, MAXITER, NONFINITE, SINGULAR, REFINE_FAIL, BAD_ITEM = 0, 1, 2, 3, 4, 5
+STATUS_NAMES = {OK: "ok", MAXITER: "maxiter", NONFINITE: "non_finite", SINGULAR: "singular", REFINE_FAIL: "refine_failed",
+                BAD_ITEM: "bad_item"}
 
 _P = C.c_void_p
 _I = C.c_int
@@ -48,6 +49,12 @@ _SIGNATURES = {
         _I,
         [_I, _I, _I, _I, _I, _P, _LL, _LL, _P, _LL, _LL, _P, _LL, _P, _LL, _P, _LL, _P, _LL, _P, _P, _P, _P, _P,
          _P, _P, _SZ, _P],
+    ),
+    "negf_batch_max_grid": (_I, [_I, _I, _I]),
+    "negf_batch_workspace_bytes": (_SZ, [_I, _I, _I, _I]),
+    "negf_batch_system_bytes": (_SZ, []),
+    "negf_batch_transmission": (
+        _I, [_P, _I, _I, _P, _P, _P, _I, _D, _I, _I, _I, _I, _P, _P, _P, _P, _SZ, _P],
     ),
     "negf_adjoint_workspace_bytes": (_SZ, [_I, _I, _I, _I]),
     "negf_rgf_adjoint_f64": (

@@ -242,6 +242,53 @@ int negf_rgf_transmission_mixed(int n_dev, int n_lead_l, int n_lead_r, int n_lay
   return 0;
 }
 
+int negf_batch_max_grid(int max_order, int precision, int blocks_per_sm) {
+  if (max_order <= 0 || max_order > 256 || (precision != 0 && precision != 1)) return 0;
+  if (blocks_per_sm != 1 && blocks_per_sm != 2) return 0;
+  const int g = negf::batch_max_grid((max_order + 15) / 16 * 16, precision, blocks_per_sm);
+  return g > 0 ? g : 0;
+}
+
+size_t negf_batch_system_bytes(void) { return sizeof(NegfBatchSystem); }
+
+size_t negf_batch_workspace_bytes(int max_order, int precision, int blocks_per_sm, int grid) {
+  const int gmax = negf_batch_max_grid(max_order, precision, blocks_per_sm);
+  if (gmax <= 0) return 0;
+  const int g = (grid <= 0 || grid > gmax) ? gmax : grid;
+  return kCounterBytes + negf::batch_ws_bytes((max_order + 15) / 16 * 16, g);
+}
+
+int negf_batch_transmission(const NegfBatchSystem* systems, int n_systems, int max_order, const int* item_system,
+                            const int* item_k, const double* item_omega, int n_items, double tol, int maxiter,
+                            int precision, int blocks_per_sm, int grid, double* t_out, int* status_out,
+                            int* iters_out, void* workspace, size_t workspace_bytes, void* stream) {
+  if (n_systems <= 0 || n_items < 0) return fail(NEGF_EINVAL, "negf_batch_transmission: bad sizes");
+  if (!systems || !item_system || !item_k || !item_omega || !t_out)
+    return fail(NEGF_EINVAL, "negf_batch_transmission: null pointer");
+  if (max_order <= 0 || max_order > 256)
+    return fail(NEGF_EUNSUPPORTED, "negf_batch_transmission: max_order must be in 1..256");
+  if (precision != 0 && precision != 1) return fail(NEGF_EINVAL, "negf_batch_transmission: precision must be 0 or 1");
+  if (maxiter <= 0 || !(tol > 0.0)) return fail(NEGF_EINVAL, "negf_batch_transmission: maxiter and tol must be positive");
+  if (blocks_per_sm != 1 && blocks_per_sm != 2)
+    return fail(NEGF_EINVAL, "negf_batch_transmission: blocks_per_sm must be 1 or 2");
+  const int gmax = negf_batch_max_grid(max_order, precision, blocks_per_sm);
+  if (gmax <= 0) return cuda_fail("negf_batch_transmission: occupancy query");
+  if (grid > gmax) return fail(NEGF_EINVAL, "negf_batch_transmission: grid above negf_batch_max_grid");
+  const int g = grid <= 0 ? gmax : grid;
+  const int npmax = (max_order + 15) / 16 * 16;
+  if (!workspace || workspace_bytes < kCounterBytes + negf::batch_ws_bytes(npmax, g))
+    return fail(NEGF_EINVAL, "negf_batch_transmission: workspace missing or too small");
+  if (n_items == 0) return 0;
+  cudaStream_t st = as_stream(stream);
+  if (cudaMemsetAsync(workspace, 0, sizeof(unsigned int), st) != cudaSuccess)
+    return cuda_fail("negf_batch_transmission: counter reset");
+  if (negf::batch_launch(systems, n_systems, item_system, item_k, item_omega, n_items, tol, maxiter, t_out,
+                         status_out, iters_out, npmax, precision, blocks_per_sm, g, workspace,
+                         static_cast<char*>(workspace) + kCounterBytes, st) != 0)
+    return cuda_fail("negf_batch_transmission");
+  return 0;
+}
+
 size_t negf_adjoint_workspace_bytes(int n_dev, int n_lead_l, int n_lead_r, int n_layers) {
   if (n_dev <= 0 || n_lead_l <= 0 || n_lead_r <= 0 || n_layers <= 0) return 0;
   const int nmax = max3(n_dev, n_lead_l, n_lead_r);

@@ -13,6 +13,7 @@ enum Status : int {
   kNonFinite = 2,   // inf/nan appeared
   kSingular = 3,    // exact zero pivot in an inversion
   kRefineFail = 4,  // mixed-precision refinement did not converge
+  kBadItem = 5,     // batch item with an out-of-range system, k index or block order
 };
 
 __device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }

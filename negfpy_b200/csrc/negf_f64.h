@@ -2,6 +2,8 @@
 #pragma once
 #include <cuda_runtime.h>
 
+struct NegfBatchSystem;  // include/negf_b200.h
+
 namespace negf {
 
 // Sancho-Rubio over a batch of points; complex matrices are interleaved
@@ -71,6 +73,13 @@ int mixed_order(int n);  // padded order (multiple of 16), 0 if unsupported
 int rgf_mixed_grid(int np);
 size_t rgf_mixed_ws_bytes(int np, int n, int grid);
 int rgf_mixed_launch(const RgfArgs& a, int np, int grid, void* ws, cudaStream_t st);
+
+// Uneven batch (negf_batch.cu).
+int batch_max_grid(int npmax, int mixed, int minb);
+size_t batch_ws_bytes(int npmax, int grid);
+int batch_launch(const ::NegfBatchSystem* sys, int n_systems, const int* item_system, const int* item_k,
+                 const double* item_omega, int n_items, double tol, int maxiter, double* t_out, int* status_out,
+                 int* iters_out, int npmax, int mixed, int minb, int grid, void* counter, void* ws, cudaStream_t st);
 
 size_t grad_ws_bytes(int np, int n, int L, int grid);
 int grad_grid(int np);

@@ -20,350 +20,19 @@
 // status; the host re-solves those points with the FP64 kernel.
 #include "negf_common.cuh"
 #include "negf_f64.h"
+#include "negf_mixed.cuh"
 #include "negf_tiles.cuh"
 
 namespace negf {
 namespace mixed {
-
-using glob::kThreads;
-using glob::kWarps;
-using glob::Tile;
-using glob::tc;
-using glob::tile_of;
-using glob::tr;
-
-__device__ __forceinline__ float2 fadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ float2 fneg(float2 a) { return make_float2(-a.x, -a.y); }
-__device__ __forceinline__ float2 fmulc(float2 a, float2 b) {
-  return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
-}
-__device__ __forceinline__ float2 to_f(double2 v) { return make_float2((float)v.x, (float)v.y); }
-
-// ------------------------------------------------------ 3 x TF32 products --
-__device__ __forceinline__ unsigned tf32_rna(float x) {
-  unsigned r;
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-  return r;
-}
-// x = hi + lo with both parts representable in TF32.
-__device__ __forceinline__ void split_tf32(float x, unsigned& hi, unsigned& lo) {
-  hi = tf32_rna(x);
-  lo = tf32_rna(x - __uint_as_float(hi));
-}
-__device__ __forceinline__ void mma_tf32(float (&d)[4], const unsigned (&a)[4], unsigned b0, unsigned b1) {
-  asm("mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
-      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
-}
-// A fragment (16 x 8) of a complex matrix, split: re/im x hi/lo.
-struct AFrag {
-  unsigned rh[4], rl[4], ih[4], il[4];
-};
-// B fragment (8 x 8): re, im and -im, each hi/lo.
-struct BFrag {
-  unsigned rh[2], rl[2], ih[2], il[2], nih[2], nil[2];
-};
-__device__ __forceinline__ void set_a(AFrag& f, int q, float2 v) {
-  split_tf32(v.x, f.rh[q], f.rl[q]);
-  split_tf32(v.y, f.ih[q], f.il[q]);
-}
-__device__ __forceinline__ void set_b(BFrag& f, int q, float2 v) {
-  split_tf32(v.x, f.rh[q], f.rl[q]);
-  split_tf32(v.y, f.ih[q], f.il[q]);
-  f.nih[q] = f.ih[q] ^ 0x80000000u;
-  f.nil[q] = f.il[q] ^ 0x80000000u;
-}
-// c += a b for one m16n8 complex tile: real = ar br - ai bi, imag = ar bi + ai br,
-// each real product as lo*hi + hi*lo + hi*hi (small terms first).
-__device__ __forceinline__ void cmma3(float (&cr)[4], float (&ci)[4], const AFrag& a, const BFrag& b) {
-  mma_tf32(cr, a.rl, b.rh[0], b.rh[1]);
-  mma_tf32(cr, a.rh, b.rl[0], b.rl[1]);
-  mma_tf32(cr, a.il, b.nih[0], b.nih[1]);
-  mma_tf32(cr, a.ih, b.nil[0], b.nil[1]);
-  mma_tf32(cr, a.rh, b.rh[0], b.rh[1]);
-  mma_tf32(cr, a.ih, b.nih[0], b.nih[1]);
-  mma_tf32(ci, a.rl, b.ih[0], b.ih[1]);
-  mma_tf32(ci, a.rh, b.il[0], b.il[1]);
-  mma_tf32(ci, a.il, b.rh[0], b.rh[1]);
-  mma_tf32(ci, a.ih, b.rl[0], b.rl[1]);
-  mma_tf32(ci, a.rh, b.ih[0], b.ih[1]);
-  mma_tf32(ci, a.ih, b.rh[0], b.rh[1]);
-}
-
-struct Acc32 {
-  float re[2][4], im[2][4];
-  __device__ __forceinline__ void zero() {
-#pragma unroll
-    for (int j = 0; j < 2; ++j)
-#pragma unroll
-      for (int q = 0; q < 4; ++q) re[j][q] = im[j][q] = 0.f;
-  }
-  __device__ __forceinline__ float2 get(int j, int q) const { return make_float2(re[j][q], im[j][q]); }
-};
-
-// acc = op(A) op(B) for one 16 x 16 tile (FP32 matrices, row stride ld),
-// contraction over kch chunks of 8; AC / BC: conjugate-transposed operand.
-template <bool AC, bool BC>
-__device__ __forceinline__ void tile_mm32(Acc32& c, const float2* __restrict__ A, const float2* __restrict__ B, int ld,
-                                          int kch, const Tile& T) {
-  c.zero();
-  for (int kc = 0; kc < kch; ++kc) {
-    const int k0 = kc * 8;
-    AFrag a;
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const int r = T.m0 + T.g + 8 * (q & 1), k = k0 + T.t + 4 * (q >> 1);
-      float2 v = AC ? A[(long long)k * ld + r] : A[(long long)r * ld + k];
-      if (AC) v.y = -v.y;
-      set_a(a, q, v);
-    }
-#pragma unroll
-    for (int j = 0; j < 2; ++j) {
-      BFrag b;
-#pragma unroll
-      for (int q = 0; q < 2; ++q) {
-        const int k = k0 + T.t + 4 * q, cc = T.n0 + 8 * j + T.g;
-        float2 v = BC ? B[(long long)cc * ld + k] : B[(long long)k * ld + cc];
-        if (BC) v.y = -v.y;
-        set_b(b, q, v);
-      }
-      // The chunk's three passes start from zero and are added with a
-      // round-to-nearest FP32 add: the tensor cores' own accumulation
-      // truncates, and accumulating every chunk inside them biases |c| low.
-      float pr[4] = {0.f, 0.f, 0.f, 0.f}, pi[4] = {0.f, 0.f, 0.f, 0.f};
-      cmma3(pr, pi, a, b);
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        c.re[j][q] = __fadd_rn(c.re[j][q], pr[q]);
-        c.im[j][q] = __fadd_rn(c.im[j][q], pi[q]);
-      }
-    }
-  }
-}
-
-// ------------------------------------------------------- FP32 Gauss-Jordan --
-// Same algorithm as glob::gj_invert_global: 8-column panels in shared memory,
-// division-free lambda-scaled elimination, look-ahead integer pivot keys (top
-// bits of max(|re|, |im|) as FP32 bit patterns, row index in the low 8 bits),
-// rank-8 update between two global buffers, final column gather.
-struct GJS32 {
-  float2* panel;
-  int* sig;
-  int* siginv;
-  int* pivlog;
-  unsigned* key;
-};
-__host__ __device__ inline size_t gjs32_bytes(int np) { return (size_t)2 * np * 8 * 8 + 3 * np * 4 + 8 * 4; }
-__device__ __forceinline__ GJS32 carve32(unsigned char* base, int np) {
-  GJS32 s;
-  s.panel = reinterpret_cast<float2*>(base);
-  s.sig = reinterpret_cast<int*>(base + (size_t)2 * np * 8 * 8);
-  s.siginv = s.sig + np;
-  s.pivlog = s.siginv + np;
-  s.key = reinterpret_cast<unsigned*>(s.pivlog + np);
-  return s;
-}
-__device__ __forceinline__ unsigned pivot_key32(float2 v, int r) {
-  const unsigned ha = __float_as_uint(v.x) & 0x7fffffffu;
-  const unsigned hb = __float_as_uint(v.y) & 0x7fffffffu;
-  const unsigned hm = ha > hb ? ha : hb;
-  return (hm & ~255u) | (unsigned)(255 - r);
-}
-// 1 / v by Smith's algorithm (R. L. Smith, CACM 5(8), 1962).
-__device__ __forceinline__ float2 crecip_smith32(float2 v) {
-  if (fabsf(v.x) >= fabsf(v.y)) {
-    const float r = v.y / v.x;
-    const float i = 1.0f / fmaf(v.y, r, v.x);
-    return make_float2(i, -r * i);
-  }
-  const float r = v.x / v.y;
-  const float i = 1.0f / fmaf(v.x, r, v.y);
-  return make_float2(r * i, -i);
-}
-
-__device__ int gj_invert32(float2* X, float2* Y, int n, int NP, const GJS32& sh, float2** out) {
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int np16 = NP >> 4, ntiles = np16 * np16;
-  const int PE = NP * 8;
-  float2* cur = X;
-  float2* nxt = Y;
-  for (int k0 = 0; k0 < n; k0 += 8) {
-    const int jmax = (n - k0) < 8 ? (n - k0) : 8;
-    float2* P = sh.panel;
-    float2* Pn = sh.panel + PE;
-    unsigned key0 = 0u;
-    for (int e = tid; e < PE; e += kThreads) {
-      const int r = e >> 3, c = e & 7;
-      const float2 v = cur[(long long)r * NP + k0 + c];
-      P[e] = v;
-      if (c == 0 && r >= k0 && r < n) key0 = max(key0, pivot_key32(v, r));
-    }
-    for (int r = tid; r < NP; r += kThreads) {
-      sh.sig[r] = r;
-      sh.siginv[r] = r;
-    }
-    if (tid < 8) sh.key[tid] = 0u;
-    __syncthreads();
-    key0 = __reduce_max_sync(0xffffffffu, key0);
-    if (lane == 0 && key0) atomicMax(&sh.key[0], key0);
-    __syncthreads();
-    float2 lam = make_float2(1.f, 0.f);
-    for (int j = 0; j < jmax; ++j) {
-      const unsigned key = sh.key[j];
-      if ((key >> 23) >= 0xffu) return kNonFinite;
-      if ((key >> 8) == 0u) return kSingular;
-      const int pr = 255 - (int)(key & 255u);
-      const int ex = (int)(key >> 23);
-      const float sc = (ex != 0 && ex < 254) ? __uint_as_float((unsigned)(254 - ex) << 23) : 1.0f;
-      if (tid == 0) {
-        const int k = k0 + j;
-        const int bl = sh.siginv[pr];
-        const int pa = sh.sig[k];
-        sh.sig[k] = pr;
-        sh.sig[bl] = pa;
-        sh.siginv[pr] = k;
-        sh.siginv[pa] = bl;
-        sh.pivlog[k] = bl;
-      }
-      const float2 piv = P[pr * 8 + j];
-      const float2 ps = make_float2(piv.x * sc, piv.y * sc);
-      unsigned nk = 0u;
-      for (int e = tid; e < PE; e += kThreads) {
-        const int r = e >> 3, c = e & 7;
-        const bool isp = (r == pr);
-        const float2 fv = P[r * 8 + j], mv = P[pr * 8 + c], av = P[e];
-        const float2 bb = isp ? fneg(lam) : fv;
-        const float2 b = make_float2(bb.x * sc, bb.y * sc);
-        const float2 m = (c == j) ? lam : mv;
-        float2 v = fneg(fmulc(b, m));
-        if (!isp && c != j) cfma(v, ps, av);
-        Pn[e] = v;
-        if (c == j + 1 && r >= k0 && r < n) {
-          bool used = isp;
-          for (int i = 0; i < j; ++i) used = used || (sh.sig[k0 + i] == r);
-          if (!used) nk = max(nk, pivot_key32(v, r));
-        }
-      }
-      lam = fmulc(lam, ps);
-      if (j + 1 < jmax) {
-        nk = __reduce_max_sync(0xffffffffu, nk);
-        if (lane == 0 && nk) atomicMax(&sh.key[j + 1], nk);
-      }
-      __syncthreads();
-      float2* t = P;
-      P = Pn;
-      Pn = t;
-    }
-    // rank-8 update of the whole matrix
-    const float2 il = crecip_smith32(lam);
-    for (int tt = warp; tt < ntiles; tt += kWarps) {
-      const Tile T = tile_of(tt, np16);
-      Acc32 c;
-      int srow[2];
-      bool inpanel[2];
-#pragma unroll
-      for (int ri = 0; ri < 2; ++ri) {
-        const int r = T.m0 + T.g + 8 * ri;
-        srow[ri] = sh.sig[r];
-        inpanel[ri] = r >= k0 && r < k0 + jmax;
-      }
-#pragma unroll
-      for (int j2 = 0; j2 < 2; ++j2)
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          const float2 v = cur[(long long)srow[q >> 1] * NP + tc(T, j2, q)];
-          c.re[j2][q] = inpanel[q >> 1] ? 0.f : v.x;
-          c.im[j2][q] = inpanel[q >> 1] ? 0.f : v.y;
-        }
-      AFrag a;
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int kk = T.t + 4 * (q >> 1);
-        set_a(a, q, fmulc(P[srow[q & 1] * 8 + kk], il));
-      }
-      const int kk0 = T.t, kk1 = T.t + 4;
-      const int pr0 = kk0 < jmax ? sh.sig[k0 + kk0] : 0, pr1 = kk1 < jmax ? sh.sig[k0 + kk1] : 0;
-#pragma unroll
-      for (int j2 = 0; j2 < 2; ++j2) {
-        const int cc = T.n0 + 8 * j2 + T.g;
-        const float2 v0 = cur[(long long)pr0 * NP + cc], v1 = cur[(long long)pr1 * NP + cc];
-        BFrag b;
-        set_b(b, 0, kk0 < jmax ? v0 : make_float2(0.f, 0.f));
-        set_b(b, 1, kk1 < jmax ? v1 : make_float2(0.f, 0.f));
-        float pr[4] = {0.f, 0.f, 0.f, 0.f}, pi[4] = {0.f, 0.f, 0.f, 0.f};
-        cmma3(pr, pi, a, b);
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          c.re[j2][q] = __fadd_rn(c.re[j2][q], pr[q]);
-          c.im[j2][q] = __fadd_rn(c.im[j2][q], pi[q]);
-        }
-      }
-#pragma unroll
-      for (int j2 = 0; j2 < 2; ++j2)
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          const int r = tr(T, q), cc = tc(T, j2, q);
-          float2 v = c.get(j2, q);
-          if (cc >= k0 && cc < k0 + 8) v = fmulc(P[srow[q >> 1] * 8 + (cc - k0)], il);
-          nxt[(long long)r * NP + cc] = v;
-        }
-    }
-    __syncthreads();
-    float2* t = cur;
-    cur = nxt;
-    nxt = t;
-  }
-  __syncthreads();
-  for (int c = tid; c < NP; c += kThreads) {
-    int s = c;
-    for (int k = 0; k < n; ++k) {
-      const int b = sh.pivlog[k];
-      s = (s == k) ? b : ((s == b) ? k : s);
-    }
-    sh.sig[c] = s;
-  }
-  __syncthreads();
-  for (long long e = tid; e < (long long)NP * NP; e += kThreads) {
-    const int r = (int)(e / NP), c = (int)(e - (long long)r * NP);
-    nxt[e] = cur[(long long)r * NP + sh.sig[c]];
-  }
-  __syncthreads();
-  *out = nxt;
-  return kOk;
-}
-
-// FP64 n x n (row stride n) -> FP32 padded NP x NP, zeros outside.
-__device__ __forceinline__ void load_pad32(float2* dst, const double2* __restrict__ src, int n, int NP) {
-  for (long long e = threadIdx.x; e < (long long)NP * NP; e += kThreads) {
-    const int r = (int)(e / NP), c = (int)(e - (long long)r * NP);
-    dst[e] = (r < n && c < n) ? to_f(src[(long long)r * n + c]) : make_float2(0.f, 0.f);
-  }
-}
-
-// ------------------------------------------------------------------ kernel --
-// Workspace per block: 4 NP x NP FP64 buffers (V / g / V g for the
-// self-energies, then Gamma_L, Gamma_R, G widened, Gamma_L G), Sigma_L and
-// Sigma_R (n x n FP64), and 6 NP x NP FP32 buffers (g_l, C, W, U, G_0, the
-// second inversion buffer).
-__host__ __device__ inline size_t mixed_ws_elems64(int np, int n) { return 4 * (size_t)np * np + 2 * (size_t)n * n; }
-__host__ __device__ inline size_t mixed_ws_bytes_per_block(int np, int n) {
-  return mixed_ws_elems64(np, n) * 16 + 6 * (size_t)np * np * 8;
-}
 
 __global__ void __launch_bounds__(kThreads) rgf_mixed_kernel(RgfArgs a, int NP, unsigned char* ws) {
   extern __shared__ __align__(16) unsigned char smraw[];
   const GJS32 sh = carve32(smraw, NP);
   double* red = reinterpret_cast<double*>(smraw + ((gjs32_bytes(NP) + 15) / 16) * 16);
   __shared__ int s_point;
-  const int n = a.n, L = a.L, tid = threadIdx.x, warp = tid >> 5;
-  const int np16 = NP >> 4, ntiles = np16 * np16, kch = (n + 7) >> 3;
-  const long long M2 = (long long)NP * NP;
+  const int n = a.n, tid = threadIdx.x;
   unsigned char* blk = ws + (long long)blockIdx.x * mixed_ws_bytes_per_block(NP, n);
-  double2* d64 = reinterpret_cast<double2*>(blk);
-  double2 *B0 = d64, *B1 = d64 + M2, *B2 = d64 + 2 * M2, *B3 = d64 + 3 * M2;
-  double2* sigL = d64 + 4 * M2;
-  double2* sigR = sigL + (long long)n * n;
-  float2* f32 = reinterpret_cast<float2*>(blk + mixed_ws_elems64(NP, n) * 16);
 
   for (;;) {
     if (tid == 0) s_point = (int)atomicAdd(a.counter, 1u);
@@ -379,180 +48,23 @@ __global__ void __launch_bounds__(kThreads) rgf_mixed_kernel(RgfArgs a, int NP, 
       }
       continue;
     }
-    float2 *pg = f32, *pc = f32 + M2, *bW = f32 + 2 * M2, *bU = f32 + 3 * M2, *bG0 = f32 + 4 * M2,
-           *bX = f32 + 5 * M2;
     const long long k = a.kidx ? (long long)a.kidx[p] : 0;
-    const double2 z = glob::z_of(a.omega[p], a.eta_dev[p]);
-    const double2* D = a.D + k * a.d_ks;
-    const double2* C = a.C + k * a.c_ks;
-
-    // FP64: Sigma = V g V^H for both contacts.
-    for (int side = 0; side < 2; ++side) {
-      const int nl = side ? a.nr : a.nl;
-      const int lch = (nl + 7) >> 3;
-      const double2* V = side ? a.VR + k * a.vr_ks : a.VL + k * a.vl_ks;
-      const double2* g = side ? a.gR + (long long)p * a.gr_ps : a.gL + (long long)p * a.gl_ps;
-      double2* S = side ? sigR : sigL;
-      glob::load_pad(B0, V, n, nl, NP, 0.0);
-      glob::load_pad(B1, g, nl, nl, NP, 0.0);
-      __syncthreads();
-      for (int tt = warp; tt < ntiles; tt += kWarps) {
-        const Tile T = tile_of(tt, np16);
-        glob::Acc c;
-        glob::tile_mm<false, false>(c, B0, NP, B1, NP, lch, T);
-#pragma unroll
-        for (int j = 0; j < 2; ++j)
-#pragma unroll
-          for (int q = 0; q < 4; ++q) B2[(long long)tr(T, q) * NP + tc(T, j, q)] = c.get(j, q);
-      }
-      __syncthreads();
-      for (int tt = warp; tt < ntiles; tt += kWarps) {
-        const Tile T = tile_of(tt, np16);
-        glob::Acc c;
-        glob::tile_mm<false, true>(c, B2, NP, B0, NP, lch, T);
-#pragma unroll
-        for (int j = 0; j < 2; ++j)
-#pragma unroll
-          for (int q = 0; q < 4; ++q) {
-            const int r = tr(T, q), cc = tc(T, j, q);
-            if (r < n && cc < n) S[r * n + cc] = c.get(j, q);
-          }
-      }
-      __syncthreads();
-    }
-    // FP32 sweep.  Layer 0: g_0 = (z - D_0 - Sigma_L [- Sigma_R when L == 1])^-1.
-    for (long long e = tid; e < M2; e += kThreads) {
-      const int r = (int)(e / NP), c = (int)(e - (long long)r * NP);
-      float2 v;
-      if (r < n && c < n) {
-        double2 w = csub(cneg(D[r * n + c]), sigL[r * n + c]);
-        if (L == 1) w = csub(w, sigR[r * n + c]);
-        if (r == c) w = cadd(w, z);
-        v = to_f(w);
-      } else {
-        v = make_float2(r == c ? 1.f : 0.f, 0.f);
-      }
-      pg[e] = v;
-    }
-    __syncthreads();
-    float2* inv = nullptr;
-    int status = gj_invert32(pg, bX, n, NP, sh, &inv);
-    if (status == kOk) {
-      if (inv != pg) {
-        bX = pg;
-        pg = inv;
-      }
-      for (long long e = tid; e < M2; e += kThreads) bG0[e] = pg[e];
-      for (int l = 1; l < L && status == kOk; ++l) {
-        load_pad32(pc, C + (long long)(l - 1) * a.c_ls, n, NP);
-        __syncthreads();
-        // W = g_{l-1} C, U = G_{0,l-1} C
-        for (int tt = warp; tt < ntiles; tt += kWarps) {
-          const Tile T = tile_of(tt, np16);
-          Acc32 c1, c2;
-          tile_mm32<false, false>(c1, pg, pc, NP, kch, T);
-          tile_mm32<false, false>(c2, bG0, pc, NP, kch, T);
-#pragma unroll
-          for (int j = 0; j < 2; ++j)
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-              const long long e = (long long)tr(T, q) * NP + tc(T, j, q);
-              bW[e] = c1.get(j, q);
-              bU[e] = c2.get(j, q);
-            }
-        }
-        __syncthreads();
-        // M = z - D_l - C^H W [- Sigma_R on the last layer] into the old g buffer;
-        // the FP64 terms are combined in FP64 before the rounding.
-        const double2* Dl = D + (long long)l * a.d_ls;
-        const bool last = (l == L - 1);
-        for (int tt = warp; tt < ntiles; tt += kWarps) {
-          const Tile T = tile_of(tt, np16);
-          Acc32 c1;
-          tile_mm32<true, false>(c1, pc, bW, NP, kch, T);
-#pragma unroll
-          for (int j = 0; j < 2; ++j)
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-              const int r = tr(T, q), cc = tc(T, j, q);
-              float2 v;
-              if (r < n && cc < n) {
-                double2 w = cneg(Dl[r * n + cc]);
-                if (last) w = csub(w, sigR[r * n + cc]);
-                if (r == cc) w = cadd(w, z);
-                v = make_float2((float)(w.x - (double)c1.re[j][q]), (float)(w.y - (double)c1.im[j][q]));
-              } else {
-                v = make_float2(r == cc ? 1.f : 0.f, 0.f);
-              }
-              pg[(long long)r * NP + cc] = v;
-            }
-        }
-        __syncthreads();
-        status = gj_invert32(pg, bX, n, NP, sh, &inv);
-        if (status != kOk) break;
-        if (inv != pg) {
-          bX = pg;
-          pg = inv;
-        }
-        // G_{0,l} = U g_l
-        for (int tt = warp; tt < ntiles; tt += kWarps) {
-          const Tile T = tile_of(tt, np16);
-          Acc32 c1;
-          tile_mm32<false, false>(c1, bU, pg, NP, kch, T);
-#pragma unroll
-          for (int j = 0; j < 2; ++j)
-#pragma unroll
-            for (int q = 0; q < 4; ++q) bG0[(long long)tr(T, q) * NP + tc(T, j, q)] = c1.get(j, q);
-        }
-        __syncthreads();
-      }
-    }
-    // FP64: Gamma_L, Gamma_R, G widened, T = Re sum (Gamma_L G Gamma_R)_ij conj(G_ij).
+    glob::RgfPoint q;
+    q.n = n;
+    q.nl = a.nl;
+    q.nr = a.nr;
+    q.L = a.L;
+    q.D = a.D + k * a.d_ks;
+    q.d_ls = a.d_ls;
+    q.C = a.C + k * a.c_ks;
+    q.c_ls = a.c_ls;
+    q.VL = a.VL + k * a.vl_ks;
+    q.VR = a.VR + k * a.vr_ks;
+    q.gL = a.gL + (long long)p * a.gl_ps;
+    q.gR = a.gR + (long long)p * a.gr_ps;
+    q.z = glob::z_of(a.omega[p], a.eta_dev[p]);
     double tval = 0.0;
-    if (status == kOk) {
-      for (long long e = tid; e < M2; e += kThreads) {
-        const int r = (int)(e / NP), c = (int)(e - (long long)r * NP);
-        double2 gl = make_double2(0.0, 0.0), gr = gl;
-        if (r < n && c < n) {
-          double2 d = csub(sigL[r * n + c], cconj(sigL[c * n + r]));
-          gl = make_double2(-d.y, d.x);
-          d = csub(sigR[r * n + c], cconj(sigR[c * n + r]));
-          gr = make_double2(-d.y, d.x);
-        }
-        B0[e] = gl;
-        B1[e] = gr;
-        const float2 gv = bG0[e];
-        B2[e] = make_double2((double)gv.x, (double)gv.y);
-      }
-      __syncthreads();
-      for (int tt = warp; tt < ntiles; tt += kWarps) {
-        const Tile T = tile_of(tt, np16);
-        glob::Acc c1;
-        glob::tile_mm<false, false>(c1, B0, NP, B2, NP, kch, T);
-#pragma unroll
-        for (int j = 0; j < 2; ++j)
-#pragma unroll
-          for (int q = 0; q < 4; ++q) B3[(long long)tr(T, q) * NP + tc(T, j, q)] = c1.get(j, q);
-      }
-      __syncthreads();
-      double t = 0.0;
-      for (int tt = warp; tt < ntiles; tt += kWarps) {
-        const Tile T = tile_of(tt, np16);
-        glob::Acc c1;
-        glob::tile_mm<false, false>(c1, B3, NP, B1, NP, kch, T);
-#pragma unroll
-        for (int j = 0; j < 2; ++j)
-#pragma unroll
-          for (int q = 0; q < 4; ++q) {
-            const double2 g = B2[(long long)tr(T, q) * NP + tc(T, j, q)];
-            t += c1.re[j][q] * g.x + c1.im[j][q] * g.y;
-          }
-      }
-      tval = block_sum(t, red);
-      if (!isfinite(tval)) status = kNonFinite;
-    } else {
-      __syncthreads();
-    }
+    const int status = rgf_point_mixed(q, NP, blk, sh, red, &tval);
     if (tid == 0) {
       a.T_out[p] = (status == kOk) ? tval : __longlong_as_double(0x7ff8000000000000ULL);
       if (a.status_out) a.status_out[p] = status;

@@ -1,6 +1,7 @@
 // Warp-tile building blocks of the global-workspace kernels: FP64 DMMA
 // complex products on 16 x 16 tiles whose fragments are loaded from
-// row-major global (L2-resident) matrices, and padded loads.  Shared by the
+// row-major global (L2-resident) matrices, padded loads, and the blocked
+// Gauss-Jordan inverse between two global buffers.  Shared by the
 // FP64 kernels and by the FP64 parts (self-energies, trace) of the
 // mixed-precision device solve.
 #pragma once
@@ -98,6 +99,204 @@ __device__ __forceinline__ void load_pad(double2* dst, const double2* __restrict
     if (r == c && (r >= nr || c >= nc)) v = make_double2(diag, 0.0);
     dst[e] = v;
   }
+}
+
+// ---------------------------------------------------------- Gauss-Jordan --
+__device__ __forceinline__ unsigned pivot_key8(double2 v, int r) {
+  const unsigned ha = (unsigned)__double2hiint(v.x) & 0x7fffffffu;
+  const unsigned hb = (unsigned)__double2hiint(v.y) & 0x7fffffffu;
+  const unsigned hm = ha > hb ? ha : hb;
+  return (hm & ~255u) | (unsigned)(255 - r);
+}
+__device__ __forceinline__ double2 crecip_smith(double2 v) {
+  if (fabs(v.x) >= fabs(v.y)) {
+    const double r = v.y / v.x;
+    const double i = 1.0 / fma(v.y, r, v.x);
+    return make_double2(i, -r * i);
+  }
+  const double r = v.x / v.y;
+  const double i = 1.0 / fma(v.x, r, v.y);
+  return make_double2(r * i, -i);
+}
+
+// Shared scratch of the inversion for order NP: panel ping-pong (2 x NP x 8),
+// permutation bookkeeping and the panel keys.
+struct GJS {
+  double2* panel;
+  int* sig;
+  int* siginv;
+  int* pivlog;
+  unsigned* key;
+};
+__host__ __device__ inline size_t gjs_bytes(int np) { return (size_t)2 * np * 8 * 16 + 3 * np * 4 + 8 * 4; }
+__device__ __forceinline__ GJS carve(unsigned char* base, int np) {
+  GJS s;
+  s.panel = reinterpret_cast<double2*>(base);
+  s.sig = reinterpret_cast<int*>(base + (size_t)2 * np * 8 * 16);
+  s.siginv = s.sig + np;
+  s.pivlog = s.siginv + np;
+  s.key = reinterpret_cast<unsigned*>(s.pivlog + np);
+  return s;
+}
+
+// Inverse of the leading n x n block of X (padding = identity), NP <= 256,
+// using Y as the second global buffer; *out is the buffer with the inverse.
+// Same algorithm as gj_invert of the shared-memory kernels (see there): the
+// n x 8 panels are factored in shared memory by the whole block with a
+// division-free lambda-scaled rule and look-ahead pivot keys (top bits of
+// max(|re|, |im|), row index in the low 8 bits: the column maximum up to a
+// relative 2^-12), the rank-8 update writes the next global buffer in the new
+// row order, and the interchanges are undone by a final column gather.
+static __device__ int gj_invert_global(double2* X, double2* Y, int n, int NP, const GJS& sh, double2** out) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int np16 = NP >> 4, ntiles = np16 * np16;
+  const int PE = NP * 8;
+  double2* cur = X;
+  double2* nxt = Y;
+  for (int k0 = 0; k0 < n; k0 += 8) {
+    const int jmax = (n - k0) < 8 ? (n - k0) : 8;
+    double2* P = sh.panel;
+    double2* Pn = sh.panel + PE;
+    unsigned key0 = 0u;
+    for (int e = tid; e < PE; e += kThreads) {
+      const int r = e >> 3, c = e & 7;
+      const double2 v = cur[(long long)r * NP + k0 + c];
+      P[e] = v;
+      if (c == 0 && r >= k0 && r < n) key0 = max(key0, pivot_key8(v, r));
+    }
+    for (int r = tid; r < NP; r += kThreads) {
+      sh.sig[r] = r;
+      sh.siginv[r] = r;
+    }
+    if (tid < 8) sh.key[tid] = 0u;
+    __syncthreads();
+    key0 = __reduce_max_sync(0xffffffffu, key0);
+    if (lane == 0 && key0) atomicMax(&sh.key[0], key0);
+    __syncthreads();
+    double2 lam = make_double2(1.0, 0.0);
+    for (int j = 0; j < jmax; ++j) {
+      const unsigned key = sh.key[j];
+      if ((key >> 20) >= 0x7ffu) return kNonFinite;
+      if ((key >> 8) == 0u) return kSingular;
+      const int pr = 255 - (int)(key & 255u);
+      const int ex = (int)(key >> 20);
+      const double sc = (ex != 0 && ex < 2046) ? __hiloint2double((2046 - ex) << 20, 0) : 1.0;
+      if (tid == 0) {
+        const int k = k0 + j;
+        const int bl = sh.siginv[pr];
+        const int pa = sh.sig[k];
+        sh.sig[k] = pr;
+        sh.sig[bl] = pa;
+        sh.siginv[pr] = k;
+        sh.siginv[pa] = bl;
+        sh.pivlog[k] = bl;
+      }
+      const double2 piv = P[pr * 8 + j];
+      const double2 ps = make_double2(piv.x * sc, piv.y * sc);
+      unsigned nk = 0u;
+      for (int e = tid; e < PE; e += kThreads) {
+        const int r = e >> 3, c = e & 7;
+        const bool isp = (r == pr);
+        // rows already used as pivots in this panel are sig[k0..k0+j]
+        const double2 fv = P[r * 8 + j], mv = P[pr * 8 + c], av = P[e];
+        const double2 bb = isp ? cneg(lam) : fv;
+        const double2 b = make_double2(bb.x * sc, bb.y * sc);
+        const double2 m = (c == j) ? lam : mv;
+        double2 v = cneg(cmul(b, m));
+        if (!isp && c != j) cfma(v, ps, av);
+        Pn[e] = v;
+        if (c == j + 1 && r >= k0 && r < n) {
+          bool used = isp;
+          for (int i = 0; i < j; ++i) used = used || (sh.sig[k0 + i] == r);
+          if (!used) nk = max(nk, pivot_key8(v, r));
+        }
+      }
+      lam = cmul(lam, ps);
+      if (j + 1 < jmax) {
+        nk = __reduce_max_sync(0xffffffffu, nk);
+        if (lane == 0 && nk) atomicMax(&sh.key[j + 1], nk);
+      }
+      __syncthreads();
+      double2* t = P;
+      P = Pn;
+      Pn = t;
+    }
+    // rank-8 update of the whole matrix
+    const double2 il = crecip_smith(lam);
+    for (int tt = warp; tt < ntiles; tt += kWarps) {
+      const Tile T = tile_of(tt, np16);
+      Acc c;
+      int srow[2];
+      bool inpanel[2];
+#pragma unroll
+      for (int ri = 0; ri < 2; ++ri) {
+        const int r = T.m0 + T.g + 8 * ri;
+        srow[ri] = sh.sig[r];
+        inpanel[ri] = r >= k0 && r < k0 + jmax;
+      }
+#pragma unroll
+      for (int j2 = 0; j2 < 2; ++j2)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const double2 v = cur[(long long)srow[q >> 1] * NP + tc(T, j2, q)];
+          c.re[j2][q] = inpanel[q >> 1] ? 0.0 : v.x;
+          c.im[j2][q] = inpanel[q >> 1] ? 0.0 : v.y;
+        }
+      double ar[4], ai[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int kk = T.t + 4 * (q >> 1);
+        const double2 v = cmul(P[srow[q & 1] * 8 + kk], il);
+        ar[q] = v.x;
+        ai[q] = v.y;
+      }
+      const int kk0 = T.t, kk1 = T.t + 4;
+      const int pr0 = kk0 < jmax ? sh.sig[k0 + kk0] : 0, pr1 = kk1 < jmax ? sh.sig[k0 + kk1] : 0;
+#pragma unroll
+      for (int j2 = 0; j2 < 2; ++j2) {
+        const int cc = T.n0 + 8 * j2 + T.g;
+        const double2 v0 = cur[(long long)pr0 * NP + cc], v1 = cur[(long long)pr1 * NP + cc];
+        double br[2], bi[2];
+        br[0] = kk0 < jmax ? v0.x : 0.0;
+        bi[0] = kk0 < jmax ? v0.y : 0.0;
+        br[1] = kk1 < jmax ? v1.x : 0.0;
+        bi[1] = kk1 < jmax ? v1.y : 0.0;
+        cmma(c.re[j2], c.im[j2], ar, ai, br, bi);
+      }
+#pragma unroll
+      for (int j2 = 0; j2 < 2; ++j2)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const int r = tr(T, q), cc = tc(T, j2, q);
+          double2 v = c.get(j2, q);
+          if (cc >= k0 && cc < k0 + 8) v = cmul(P[srow[q >> 1] * 8 + (cc - k0)], il);
+          nxt[(long long)r * NP + cc] = v;
+        }
+    }
+    __syncthreads();
+    double2* t = cur;
+    cur = nxt;
+    nxt = t;
+  }
+  // Column map: column c of the inverse = column t_{n-1}(...t_0(c)) of cur.
+  // pivlog holds the partners; build the map for every column at once.
+  __syncthreads();
+  for (int c = tid; c < NP; c += kThreads) {
+    int s = c;
+    for (int k = 0; k < n; ++k) {
+      const int b = sh.pivlog[k];
+      s = (s == k) ? b : ((s == b) ? k : s);
+    }
+    sh.sig[c] = s;
+  }
+  __syncthreads();
+  for (long long e = tid; e < (long long)NP * NP; e += kThreads) {
+    const int r = (int)(e / NP), c = (int)(e - (long long)r * NP);
+    nxt[e] = cur[(long long)r * NP + sh.sig[c]];
+  }
+  __syncthreads();
+  *out = nxt;
+  return kOk;
 }
 
 }  // namespace glob

@@ -238,3 +238,35 @@ def subsample(wl: Workload, omega_idx, k_idx) -> Workload:
                     wl.onsite[ki], wl.coupling[ki], wl.n_layers, wl.eta, wl.eta_device, wl.omega_max,
                     wl.omega_unit_rad_s, wl.same_leads, wl.uniform_layers,
                     None if wl.vl is None else wl.vl[ki], None if wl.vr is None else wl.vr[ki], dict(wl.meta))
+
+
+# Block orders of the uneven batch and the (ny, nz) atom grid of each (3 DOF per atom).
+UNEVEN_SHAPES = {24: (2, 4), 48: (4, 4), 72: (4, 6), 96: (4, 8), 120: (4, 10), 192: (8, 8)}
+
+
+def uneven_workload(seed: int = 5, n_systems: int = 64, n_omega: int = 1024, k_range: tuple[int, int] = (1, 256),
+                    layer_range: tuple[int, int] = (10, 60), orders=tuple(UNEVEN_SHAPES)) -> list[Workload]:
+    """Independent systems for one uneven batch: block orders drawn uniformly
+    from ``orders``, lengths uniformly from ``layer_range`` layers and 1D k
+    lines of ``k_range`` points, each a seeded NN+NNN spring network (slab,
+    periodic in y) with its own omega grid of ``n_omega`` points up to
+    1.05 omega_max and eta = 1e-6 omega_max^2.  Leads are the device material
+    (identical layers)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n_systems):
+        n = int(rng.choice(orders))
+        L = int(rng.integers(layer_range[0], layer_range[1] + 1))
+        K = int(rng.integers(k_range[0], k_range[1] + 1))
+        ny, nz = UNEVEN_SHAPES[n]
+        params = spring_network(seed * 1000 + i, ny=ny, nz=nz, periodic_y=True, periodic_z=False)
+        kps = kgrid(K)
+        wmax = estimate_omega_max(params, nk=4, two_d=False)
+        st = material_kspace_stack(params, kps, n_layers=1)
+        lead = {"d00": st["d00"], "d01": st["d01"], "d10": st["d10"]}
+        om = (np.arange(n_omega, dtype=float) + 1.0) * (1.05 * wmax / n_omega)
+        out.append(Workload("uneven%d_n%d_L%d_K%d_W%d" % (i, n, L, K, n_omega), om, kps, lead, lead, st["onsite"],
+                            st["d01"][:, None], L, eta=1e-6 * wmax * wmax, omega_max=wmax,
+                            omega_unit_rad_s=omega_unit_for(wmax), uniform_layers=True,
+                            meta={"seed": seed * 1000 + i, "ny": ny, "nz": nz}))
+    return out

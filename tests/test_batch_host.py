@@ -1,0 +1,71 @@
+"""Host logic of the uneven batch (no GPU): the ctypes table layout against
+the library's own sizeof, the item orders, the autotuner's selection and
+cache, and the uneven workload generator."""
+
+from __future__ import annotations
+
+import ctypes as C
+import json
+
+import numpy as np
+import pytest
+
+from negfpy_b200 import _lib, workloads as W
+from negfpy_b200.autotune import BatchTuner, batch_signature
+from negfpy_b200.batch import NegfBatchSystem, item_cost, item_order
+
+
+def test_table_record_matches_the_c_struct():
+    lib = _lib.load()
+    assert C.sizeof(NegfBatchSystem) == int(lib.negf_batch_system_bytes())
+    assert NegfBatchSystem.onsite.offset == 24 and NegfBatchSystem.eta_device.offset == C.sizeof(NegfBatchSystem) - 8
+
+
+def test_item_orders():
+    system = np.array([0, 0, 0, 1, 1, 2])
+    cost = np.array([1.0, 1.0, 1.0, 5.0, 5.0, 3.0])
+    assert list(item_order(system, cost, "lpt")) == [3, 4, 5, 0, 1, 2]
+    assert list(item_order(system, cost, "system")) == [0, 1, 2, 3, 4, 5]
+    assert list(item_order(system, cost, "interleave")) == [0, 3, 5, 1, 4, 2]
+    with pytest.raises(ValueError):
+        item_order(system, cost, "random")
+    assert item_cost(96, 96, 96, 40, True) > item_cost(48, 48, 48, 40, True) > 0
+    assert item_cost(72, 48, 72, 30, False) > item_cost(72, 48, 72, 30, True)
+
+
+def test_tuner_selects_the_fastest_and_caches(tmp_path):
+    path = tmp_path / "tune.json"
+    tuner = BatchTuner(path)
+    times = {(1, "lpt"): 5.0, (1, "interleave"): 6.0, (1, "system"): 9.0, (2, "lpt"): 4.0,
+             (2, "interleave"): float("inf"), (2, "system"): 7.0}
+    calls = []
+
+    def measure(bps, order):
+        calls.append((bps, order))
+        if np.isinf(times[(bps, order)]):
+            raise RuntimeError("shape not available")
+        return times[(bps, order)]
+
+    key = batch_signature([(48, 48, 48, 20, 64, 1)], "f64", "gpu")
+    r = tuner.select(key, measure)
+    assert (r["blocks_per_sm"], r["order"], r["cached"]) == (2, "lpt", False)
+    assert len(calls) == 6
+    assert json.loads(path.read_text())[key]["order"] == "lpt"
+    r2 = BatchTuner(path).select(key, measure)
+    assert r2["cached"] and len(calls) == 6
+    r3 = tuner.select(key, measure, force=True)
+    assert not r3["cached"] and len(calls) == 12
+    assert batch_signature([(1, 1, 1, 2, 3, 1), (4, 4, 4, 5, 6, 1)], "f64", "g") == \
+        batch_signature([(4, 4, 4, 5, 6, 1), (1, 1, 1, 2, 3, 1)], "f64", "g")
+    with pytest.raises(RuntimeError):
+        BatchTuner(tmp_path / "x.json").select("k", lambda b, o: float("inf"))
+
+
+def test_uneven_workload_shapes():
+    ws = W.uneven_workload(seed=3, n_systems=6, n_omega=16, k_range=(1, 9), layer_range=(10, 60))
+    assert len(ws) == 6
+    for w in ws:
+        assert w.n in W.UNEVEN_SHAPES and 10 <= w.n_layers <= 60 and 1 <= len(w.kpoints) <= 9
+        assert w.omegas.size == 16 and w.omegas.max() <= 1.05 * w.omega_max + 1e-12
+        d = w.lead_l["d00"][0]
+        assert np.abs(d - d.conj().T).max() < 1e-12
