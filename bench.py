@@ -48,6 +48,9 @@ def _args():
                     help="omegas per rank (default: the full 2048; smaller values are profiling cases)")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the refined-precision and gradient measurements (run at N=1 only)")
+    ap.add_argument("--case", default="slab", choices=["slab", "bulk", "grad", "batch"],
+                    help="slab: the benchmark; bulk / grad / batch: one small launch of each kernel family "
+                         "(FP64 and mixed device solve at n=96, the adjoint, the uneven batch) for profiling")
     ap.add_argument("--kernels-only", action="store_true",
                     help="time the kernels only (no e2e, CPU baseline or peak probe); for profiling runs")
     return ap.parse_args()
@@ -323,6 +326,64 @@ def uneven_batch(torch, omega_stride=256):
             "launch": "one persistent kernel per solve, replayed from a CUDA graph; shape and order autotuned"}
 
 
+def profile_case(name, torch):
+    """One small launch of each kernel of a family (for ncu), with CUDA-event times."""
+    from negfpy_b200 import engine, spectrum, workloads as Wm
+
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+    out = {"case": name}
+    if name == "bulk":
+        wl = Wm.bulk_workload()
+        s = engine.StackedSystem.from_arrays(wl.lead_l, wl.lead_l, wl.onsite, wl.coupling, wl.n_layers)
+        wi = np.arange(3, wl.omegas.size, 256)
+        K = len(wl.kpoints)
+        om_w = torch.tensor(wl.omegas[wi], dtype=torch.float64, device="cuda")
+        w_idx, k_idx = spectrum.grid_points(len(wi), K, om_w.device)
+        om = om_w[w_idx].contiguous()
+        eta = torch.full_like(om, wl.eta)
+        e = [ev() for _ in range(4)]
+        e[0].record()
+        rl = engine.sgf_sr(*s.lead_l, om, eta, k_idx)
+        e[1].record()
+        engine.rgf_transmission(s.onsite, s.coupling, s.n_layers, s.vl, s.vr, rl["g"], rl["g"], om, eta, k_idx,
+                                rl["status"])
+        e[2].record()
+        engine.rgf_transmission(s.onsite, s.coupling, s.n_layers, s.vl, s.vr, rl["g"], rl["g"], om, eta, k_idx,
+                                rl["status"], precision="mixed")
+        e[3].record()
+        torch.cuda.synchronize()
+        out.update(points=int(om.numel()), sr_ms=e[0].elapsed_time(e[1]), rgf_f64_ms=e[1].elapsed_time(e[2]),
+                   rgf_mixed_ms=e[2].elapsed_time(e[3]))
+    elif name == "grad":
+        from negfpy_b200 import adjoint
+
+        pr = adjoint.hetero_problem(n_k=4, n_omega=32)
+        theta = torch.as_tensor(pr.model.theta0, device="cuda")
+        e = [ev() for _ in range(3)]
+        e[0].record()
+        pr.transmission(theta)
+        e[1].record()
+        pr.kappa_and_grad(theta)
+        e[2].record()
+        torch.cuda.synchronize()
+        out.update(points=pr.W * pr.K, forward_ms=e[0].elapsed_time(e[1]), grad_ms=e[1].elapsed_time(e[2]))
+    elif name == "batch":
+        from negfpy_b200.batch import UnevenBatch
+
+        ws = Wm.uneven_workload(n_systems=16, k_range=(1, 32))
+        b = UnevenBatch(ws)
+        it = b.items([w.omegas[100::200] for w in ws], "lpt")
+        for prec in ("f64", "mixed"):
+            e0, e1 = ev(), ev()
+            e0.record()
+            b.launch(it, prec, blocks_per_sm=2)
+            e1.record()
+            torch.cuda.synchronize()
+            out[prec + "_ms"] = e0.elapsed_time(e1)
+        out["items"] = int(it.system.numel())
+    print(json.dumps(out), flush=True)
+
+
 def run_reference(args):
     ws, rank, _ = _dist()
     if rank != 0:
@@ -361,6 +422,10 @@ def main():
     if args.impl == "reference":
         return run_reference(args)
     import torch
+
+    if args.case != "slab":
+        torch.cuda.set_device(0)
+        return profile_case(args.case, torch)
     import torch.distributed as dist
 
     ws, rank, local = _dist()
@@ -486,7 +551,7 @@ def main():
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cores = os.cpu_count() or 1
-        nsamp = args.cpu_sample or max(32 * cores, 256)
+        nsamp = args.cpu_sample or max(256 * cores, 2048)
         rate, dt = cpu_rate(wl, shard, nsamp, cores)
         cpu = {"value": rate, "unit": "points/s", "cores": cores, "kind": "port",
                "sample": f"{nsamp} random points of the {W}x{K} grid ({dt:.1f} s wall); negfpy's algorithm "
