@@ -232,12 +232,12 @@ def grad_vs_forward(torch, n_k=8, n_omega=256, reps=3):
     e[1].record()
     torch.cuda.synchronize()
     theta = torch.as_tensor(pr.model.theta0, device="cuda")
-    pr.kappa_of_t(pr.transmission(theta))
+    pr.kappa_of_t(pr.transmission_theta(theta))
     pr.kappa_and_grad(theta)
     torch.cuda.synchronize()
     e[2].record()
     for _ in range(reps):
-        pr.kappa_of_t(pr.transmission(theta))
+        pr.kappa_of_t(pr.transmission_theta(theta))
     e[3].record()
     torch.cuda.synchronize()
     fwd = e[2].elapsed_time(e[3]) / reps
@@ -248,11 +248,13 @@ def grad_vs_forward(torch, n_k=8, n_omega=256, reps=3):
     g1.record()
     torch.cuda.synchronize()
     grad = g0.elapsed_time(g1) / reps
-    return {"workload": f"heterojunction lead48|L30 n72|lead72, 2000 params, {n_omega} omega x {n_k} k",
+    return {"workload": f"heterojunction lead48|L30 n72|lead72, 2000 spring params + 720 site masses, "
+                        f"{n_omega} omega x {n_k} k",
             "forward_ms": fwd, "grad_ms": grad, "grad_over_forward": grad / fwd,
             "lead_sgf_ms_once": e[0].elapsed_time(e[1]),
-            "note": "forward = theta -> blocks -> device solve -> kappa; grad = the adjoint kernel (forward "
-                    "sweeps recomputed inside) + contraction to theta; lead GFs do not depend on theta"}
+            "note": "forward = theta -> blocks -> device solve -> kappa; grad = dkappa/dtheta and dkappa/dmasses "
+                    "from one adjoint launch (forward sweeps recomputed inside) + autograd through the block "
+                    "builder; lead GFs do not depend on theta"}
 
 
 def uneven_batch(torch, omega_stride=256):
@@ -361,7 +363,7 @@ def profile_case(name, torch):
         theta = torch.as_tensor(pr.model.theta0, device="cuda")
         e = [ev() for _ in range(3)]
         e[0].record()
-        pr.transmission(theta)
+        pr.transmission_theta(theta)
         e[1].record()
         pr.kappa_and_grad(theta)
         e[2].record()

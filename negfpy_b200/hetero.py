@@ -16,9 +16,10 @@ The device is described bond by bond.  A set of bonds around the interface
 are parameters: ``theta`` (FP64) overrides their spring constants, and the
 blocks are linear in theta:
     D(k; theta) = D_fixed(k) + sum_p theta_p dD(k)/dtheta_p.
-``blocks(theta)`` evaluates them on the GPU with torch (differentiable for
-a dense check), ``contract(grad_onsite, grad_coupling)`` turns the adjoint
-blocks of ``negf_rgf_adjoint_f64`` into dkappa/dtheta.
+``blocks(theta, kpoints, masses)`` evaluates them with torch, differentiable
+in theta and in the device site masses (D = M^-1/2 Phi M^-1/2, the pinning
+pin / m included), so gradients reach both through torch autograd from the
+block gradients that the adjoint kernel provides.
 """
 
 from __future__ import annotations
@@ -34,14 +35,17 @@ from .workloads import _half_space_neighbours
 
 @dataclass
 class Contrib:
-    """One 3x3 contribution of a bond to a block, per unit spring constant."""
+    """One 3x3 contribution of a bond to a block, per unit spring constant
+    and before mass weighting: the block gets spring * raw / sqrt(m_a m_b)."""
 
     kind: np.ndarray    # 0 onsite block, 1 coupling block
     layer: np.ndarray   # block layer
     row: np.ndarray     # first DOF row
     col: np.ndarray     # first DOF column
     phase: np.ndarray   # transverse cell shift multiplying i ky
-    coef: np.ndarray    # [m, 3, 3] real: sign * e e^T / sqrt(m_a m_b)
+    raw: np.ndarray     # [m, 3, 3] real: +e e^T (self term) or -e e^T (pair term)
+    ma: np.ndarray      # flat index (layer * n_sites + site) of the row site's mass
+    mb: np.ndarray      # flat index of the column site's mass
     bond: np.ndarray    # bond index
 
 
@@ -135,7 +139,8 @@ class HeteroModel:
 
     # ---------------------------------------------------------------- blocks
     def _contributions(self) -> Contrib:
-        kind, layer, row, col, phase, coef, bond = [], [], [], [], [], [], []
+        kind, layer, row, col, phase, raw, ma, mb, bond = [], [], [], [], [], [], [], [], []
+        ns = self.n_sites
         for i in range(self.bond_k0.size):
             la, a, lb, b = self.bond_la[i], self.bond_a[i], self.bond_lb[i], self.bond_b[i]
             e = self.bond_e[i]
@@ -146,45 +151,43 @@ class HeteroModel:
             for (inside, l, s) in ((inside_a, la, a), (inside_b, lb, b)):
                 if inside:
                     kind.append(0), layer.append(l), row.append(3 * s), col.append(3 * s), phase.append(0)
-                    coef.append(ee / self.mass[l, s]), bond.append(i)
+                    raw.append(ee), ma.append(l * ns + s), mb.append(l * ns + s), bond.append(i)
             if not (inside_a and inside_b):
                 continue
-            ma, mb = self.mass[la, a], self.mass[lb, b]
-            w = -ee / np.sqrt(ma * mb)
+            ia, ib = la * ns + a, lb * ns + b
             if la == lb:
                 kind += [0, 0]
                 layer += [la, la]
                 row += [3 * a, 3 * b]
                 col += [3 * b, 3 * a]
                 phase += [c, -c]
-                coef += [w, w]
+                raw += [-ee, -ee]
+                ma += [ia, ib]
+                mb += [ib, ia]
                 bond += [i, i]
             else:
                 kind.append(1), layer.append(la), row.append(3 * a), col.append(3 * b), phase.append(c)
-                coef.append(w), bond.append(i)
+                raw.append(-ee), ma.append(ia), mb.append(ib), bond.append(i)
         return Contrib(np.array(kind), np.array(layer), np.array(row), np.array(col), np.array(phase, float),
-                       np.array(coef), np.array(bond))
+                       np.array(raw), np.array(ma), np.array(mb), np.array(bond))
 
-    def _pinning(self) -> np.ndarray:
-        on = np.zeros((self.L, self.n, self.n))
-        for l in range(self.L):
-            for s in range(self.n_sites):
-                if not self.active[l, s]:
-                    on[l, 3 * s:3 * s + 3, 3 * s:3 * s + 3] = np.eye(3) * self.pin / self.mass[l, s]
-        return on
-
-    def blocks(self, theta: torch.Tensor, kpoints, device=None):
-        """(onsite [K, L, n, n], coupling [K, L-1, n, n]) complex128 for spring values theta."""
+    def blocks(self, theta: torch.Tensor, kpoints, masses: torch.Tensor | None = None, device=None):
+        """(onsite [K, L, n, n], coupling [K, L-1, n, n]) complex128 for spring
+        values theta and device site masses ``masses`` ``[L, ny*nz]`` (default
+        the model's); differentiable in both with torch autograd."""
         dev = device or theta.device
         ky = torch.as_tensor(np.array([k[0] for k in kpoints], float), device=dev)
         K, L, n = ky.numel(), self.L, self.n
+        m = torch.as_tensor(self.mass, device=dev, dtype=torch.float64) if masses is None else masses.to(dev)
+        mflat = m.reshape(-1)
         kvals = torch.as_tensor(self.bond_k0, device=dev, dtype=torch.float64).clone()
         kvals = kvals.index_put((torch.as_tensor(self.param_bonds, device=dev),), theta.to(dev))
         ct = self.contrib
         spring = kvals[torch.as_tensor(ct.bond, device=dev)]                      # [m]
+        inv = torch.rsqrt(mflat[torch.as_tensor(ct.ma, device=dev)] * mflat[torch.as_tensor(ct.mb, device=dev)])
         ph = torch.exp(1j * ky[:, None] * torch.as_tensor(ct.phase, device=dev)[None, :])  # [K, m]
-        val = (spring[None, :, None, None] * ph[:, :, None, None]
-               * torch.as_tensor(ct.coef, device=dev)[None])                        # [K, m, 3, 3]
+        val = ((spring * inv)[None, :, None, None] * ph[:, :, None, None]
+               * torch.as_tensor(ct.raw, device=dev)[None])                         # [K, m, 3, 3]
         onsite = torch.zeros((K, L * n * n), dtype=torch.complex128, device=dev)
         coupling = torch.zeros((K, max(L - 1, 1) * n * n), dtype=torch.complex128, device=dev)
         ar = torch.arange(3, device=dev)
@@ -198,37 +201,16 @@ class HeteroModel:
             if bool(sel.any()):
                 idx = flat[sel].reshape(-1)
                 tgt.index_add_(1, idx, val[:, sel].reshape(K, -1))
-        onsite = onsite.reshape(K, L, n, n) + torch.as_tensor(self._pinning(), device=dev)[None]
+        # stiff pinning of the padding sites: pin / m on their 3 x 3 diagonal
+        pl, ps = np.nonzero(~self.active)
+        pin_val = self.pin / m[torch.as_tensor(pl, device=dev), torch.as_tensor(ps, device=dev)]   # [p]
+        d = torch.arange(3, device=dev)
+        idx = (torch.as_tensor(pl, device=dev)[:, None] * n * n
+               + (3 * torch.as_tensor(ps, device=dev)[:, None] + d[None, :]) * (n + 1))          # [p, 3]
+        pin_flat = torch.zeros(L * n * n, dtype=torch.float64, device=dev).index_add(
+            0, idx.reshape(-1), pin_val[:, None].expand(-1, 3).reshape(-1))
+        onsite = onsite.reshape(K, L, n, n) + pin_flat.reshape(L, n, n)[None]
         return onsite, coupling.reshape(K, max(L - 1, 1), n, n)
-
-    def contract(self, grad_onsite: torch.Tensor, grad_coupling: torch.Tensor, kpoints) -> torch.Tensor:
-        """dkappa/dtheta = 2 Re sum_k Tr[dD/dtheta X] from the accumulated adjoint blocks."""
-        dev = grad_onsite.device
-        ky = torch.as_tensor(np.array([k[0] for k in kpoints], float), device=dev)
-        K, L, n = ky.numel(), self.L, self.n
-        ct = self.contrib
-        sel = torch.as_tensor(self.is_param[ct.bond], device=dev)
-        ar = torch.arange(3, device=dev)
-        # Tr[dD X] = sum_ab dD_ab X_ba: gather X at the transposed positions
-        r = torch.as_tensor(ct.row, device=dev)[:, None, None] + ar[None, :, None]
-        c = torch.as_tensor(ct.col, device=dev)[:, None, None] + ar[None, None, :]
-        lay = torch.as_tensor(ct.layer, device=dev)[:, None, None]
-        flat_t = (lay * n * n + c * n + r)                                         # X[b, a]
-        kind = torch.as_tensor(ct.kind, device=dev)
-        ph = torch.exp(1j * ky[:, None] * torch.as_tensor(ct.phase, device=dev)[None, :])
-        coef = torch.as_tensor(ct.coef, device=dev)
-        out = torch.zeros(self.param_bonds.size, dtype=torch.float64, device=dev)
-        pmap = torch.full((self.bond_k0.size,), -1, dtype=torch.long, device=dev)
-        pmap[torch.as_tensor(self.param_bonds, device=dev)] = torch.arange(self.param_bonds.size, device=dev)
-        for kd, src in ((0, grad_onsite.reshape(K, -1)), (1, grad_coupling.reshape(K, -1))):
-            m = sel & (kind == kd)
-            if not bool(m.any()):
-                continue
-            x = src[:, flat_t[m].reshape(-1)].reshape(K, -1, 3, 3)                # [K, mm, 3, 3]
-            t = (coef[m][None] * x).sum(dim=(2, 3)) * ph[:, m]                    # [K, mm]
-            contrib = 2.0 * t.sum(dim=0).real
-            out.index_add_(0, pmap[torch.as_tensor(ct.bond, device=dev)[m]], contrib)
-        return out
 
     # ------------------------------------------------------------ the leads
     def lead_blocks(self, material: str, kpoints) -> dict:

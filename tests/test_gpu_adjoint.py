@@ -1,10 +1,12 @@
-"""Adjoint of the device solve: dkappa/dtheta and T vector-Jacobian products.
+"""Adjoint of the device solve: dkappa/dtheta, dkappa/dmasses and T
+vector-Jacobian products.
 
 Checked three ways: against torch autograd through a dense solve of the whole
 device matrix (block order n = 24, the same lead surface GFs), against central
-finite differences (h = 1e-6) of the forward kernels on 50 random parameters
-of the heterojunction (lead 48 | 30 layers of order 72 | lead 72, 2000
-parameters), and T of the heterojunction against the oracle.
+finite differences (h = 1e-6) of the forward kernels on 50 random spring
+parameters and 20 random site masses of the heterojunction (lead 48 | 30
+layers of order 72 | lead 72, 2000 spring parameters), and T of the
+heterojunction against the oracle.
 """
 
 from __future__ import annotations
@@ -19,10 +21,10 @@ from negfpy_b200 import adjoint  # noqa: E402
 from negfpy_b200.hetero import HeteroModel  # noqa: E402
 
 
-def dense_transmission(problem, theta):
+def dense_transmission(problem, theta, masses=None):
     """T[W, K] by a dense solve of A = (w + i eta)^2 - D - Sigma over all layers (torch, differentiable)."""
     m = problem.model
-    on, cp = m.blocks(theta, problem.kpoints)
+    on, cp = m.blocks(theta, problem.kpoints, masses)
     K, L, n = on.shape[0], m.L, m.n
     N = L * n
     D = torch.zeros((K, N, N), dtype=torch.complex128, device=on.device)
@@ -38,10 +40,10 @@ def dense_transmission(problem, theta):
     z = (problem.omega + 1j * problem.eta) ** 2
     eye = torch.eye(N, dtype=torch.complex128, device=on.device)
     A = z[:, None, None] * eye - D[ki]
-    pad_l = torch.zeros_like(A)
-    pad_l[:, :n, :n] = sl
-    pad_l[:, N - n:, N - n:] = sr
-    A = A - pad_l
+    pad = torch.zeros_like(A)
+    pad[:, :n, :n] = sl
+    pad[:, N - n:, N - n:] = sr
+    A = A - pad
     rhs = eye[:, N - n:].expand(A.shape[0], N, n)
     g = torch.linalg.solve(A, rhs)[:, :n, :]
     gam_l = 1j * (sl - sl.conj().transpose(-1, -2))
@@ -59,27 +61,36 @@ def small():
     return adjoint.HeteroKappaProblem(model, kp, om, 1e-6 * wmax * wmax, 300.0, 2 * np.pi * 15e12 / wmax)
 
 
+def _rel(a, b):
+    return float((a - b).abs().max()) / float(b.abs().max())
+
+
 def test_small_forward_matches_dense(small):
     theta = torch.as_tensor(small.model.theta0, device="cuda")
-    t_gpu = small.transmission(theta)
+    t_gpu = small.transmission_theta(theta)
     t_ref = dense_transmission(small, theta)
     assert float(t_ref.abs().max()) > 0.5
     err = float(((t_gpu - t_ref).abs() / t_ref.abs().clamp_min(1.0)).max())
     assert err < 1e-10, err
 
 
-def test_kappa_grad_matches_dense_autograd(small):
+def test_kappa_grads_match_dense_autograd(small):
     theta = torch.as_tensor(small.model.theta0, device="cuda").clone().requires_grad_(True)
-    kap = adjoint.kappa(theta, small)
-    (g_adj,) = torch.autograd.grad(kap, theta)
-    theta_d = theta.detach().clone().requires_grad_(True)
-    kap_d = small.kappa_of_t(dense_transmission(small, theta_d))
-    (g_ref,) = torch.autograd.grad(kap_d, theta_d)
+    masses = torch.as_tensor(small.model.mass, device="cuda").clone().requires_grad_(True)
+    kap = adjoint.kappa(theta, small, masses)
+    g_th, g_m = torch.autograd.grad(kap, [theta, masses])
+    th_d = theta.detach().clone().requires_grad_(True)
+    m_d = masses.detach().clone().requires_grad_(True)
+    kap_d = small.kappa_of_t(dense_transmission(small, th_d, m_d))
+    r_th, r_m = torch.autograd.grad(kap_d, [th_d, m_d])
     assert abs(float(kap.detach() - kap_d.detach())) <= 1e-10 * abs(float(kap_d.detach()))
-    scale = float(g_ref.abs().max())
-    assert scale > 0
-    err = float((g_adj - g_ref).abs().max()) / scale
-    assert err < 1e-9, err
+    assert float(r_th.abs().max()) > 0 and float(r_m.abs().max()) > 0
+    assert _rel(g_th, r_th) < 1e-9
+    assert _rel(g_m, r_m) < 1e-9
+    # the one-launch path gives the same gradients
+    k2, d_th, d_m = small.kappa_and_grad(theta.detach(), masses.detach())
+    assert abs(float(k2 - kap_d.detach())) <= 1e-10 * abs(float(kap_d.detach()))
+    assert _rel(d_th, r_th) < 1e-9 and _rel(d_m, r_m) < 1e-9
 
 
 def test_vjp_random_weights_matches_dense_autograd(small):
@@ -88,19 +99,20 @@ def test_vjp_random_weights_matches_dense_autograd(small):
         small.model.theta0.size, generator=gen, dtype=torch.float64).cuda())
     w = torch.randn((small.W, small.K), generator=gen, dtype=torch.float64).cuda()
     th = theta.clone().requires_grad_(True)
-    t = adjoint.TransmissionFunction.apply(th, small)
+    on, cp = small.blocks(th)
+    t = adjoint.TransmissionFunction.apply(on, cp, small)
     (g_adj,) = torch.autograd.grad(t, th, grad_outputs=w)
     th_d = theta.clone().requires_grad_(True)
     (g_ref,) = torch.autograd.grad(dense_transmission(small, th_d), th_d, grad_outputs=w)
-    err = float((g_adj - g_ref).abs().max()) / float(g_ref.abs().max())
-    assert err < 1e-9, err
+    assert _rel(g_adj, g_ref) < 1e-9
 
 
 def test_zero_weights_give_zero_gradient(small):
     theta = torch.as_tensor(small.model.theta0, device="cuda")
-    t, g = small.vjp(theta, torch.zeros((small.W, small.K), dtype=torch.float64, device="cuda"))
-    assert float(g.abs().max()) == 0.0
-    t_fwd = small.transmission(theta)
+    on, cp = small.blocks(theta)
+    t, x_on, x_cp = small.vjp(on, cp, torch.zeros((small.W, small.K), dtype=torch.float64, device="cuda"))
+    assert float(x_on.abs().max()) == 0.0 and float(x_cp.abs().max()) == 0.0
+    t_fwd = small.transmission(on, cp)
     assert float((t - t_fwd).abs().max()) < 1e-11
 
 
@@ -114,7 +126,7 @@ def test_hetero_forward_matches_oracle(hetero):
 
     m = hetero.model
     theta = torch.as_tensor(m.theta0, device="cuda")
-    t = hetero.transmission(theta).cpu().numpy()
+    t = hetero.transmission_theta(theta).cpu().numpy()
     on, cp = m.blocks(theta, hetero.kpoints)
     on, cp = on.cpu().numpy(), cp.cpu().numpy()
     la = m.lead_blocks("A", hetero.kpoints)
@@ -129,27 +141,36 @@ def test_hetero_forward_matches_oracle(hetero):
         assert abs(t[wi, ki] - ref) <= 1e-10 * max(1.0, abs(ref)), (wi, ki, t[wi, ki], ref)
 
 
-def test_hetero_grad_matches_central_differences(hetero):
+def test_hetero_grads_match_central_differences(hetero):
     m = hetero.model
     assert m.n == 72 and m.n_a == 48 and m.L == 30 and m.theta0.size == 2000
     theta = torch.as_tensor(m.theta0, device="cuda")
-    kap, g = hetero.kappa_and_grad(theta)
-    rng = np.random.default_rng(5)
-    sel = rng.choice(m.theta0.size, size=50, replace=False)
+    masses = torch.as_tensor(m.mass, device="cuda")
+    kap, g_th, g_m = hetero.kappa_and_grad(theta, masses)
     h = 1e-6
+    kap_of = lambda th, ms: float(hetero.kappa_of_t(hetero.transmission_theta(th, ms)))  # noqa: E731
+    rng = np.random.default_rng(5)
+    # spring constants
+    sel = rng.choice(m.theta0.size, size=50, replace=False)
     fd = []
     for p in sel:
-        tp = theta.clone()
-        tm = theta.clone()
+        tp, tm = theta.clone(), theta.clone()
         tp[p] += h
         tm[p] -= h
-        fd.append(float(hetero.kappa_of_t(hetero.transmission(tp)) - hetero.kappa_of_t(hetero.transmission(tm)))
-                  / (2 * h))
-    fd = np.array(fd)
-    ga = g.cpu().numpy()[sel]
-    scale = np.abs(g.cpu().numpy()).max()
-    err = np.abs(fd - ga) / scale
-    assert scale > 0
-    assert float(err.max()) < 1e-5, (float(err.max()), fd[:5], ga[:5])
-    kap_fwd = hetero.kappa_of_t(hetero.transmission(theta))
-    assert abs(float(kap - kap_fwd)) <= 1e-11 * abs(float(kap_fwd))
+        fd.append((kap_of(tp, masses) - kap_of(tm, masses)) / (2 * h))
+    ga = g_th.cpu().numpy()
+    err = np.abs(np.array(fd) - ga[sel]) / np.abs(ga).max()
+    assert float(err.max()) < 1e-5, float(err.max())
+    # site masses of the active device sites
+    act = np.flatnonzero(m.active.ravel())
+    msel = rng.choice(act, size=20, replace=False)
+    fdm = []
+    for q in msel:
+        mp, mm = masses.clone().reshape(-1), masses.clone().reshape(-1)
+        mp[q] += h
+        mm[q] -= h
+        fdm.append((kap_of(theta, mp.reshape(masses.shape)) - kap_of(theta, mm.reshape(masses.shape))) / (2 * h))
+    gm = g_m.reshape(-1).cpu().numpy()
+    errm = np.abs(np.array(fdm) - gm[msel]) / np.abs(gm).max()
+    assert float(errm.max()) < 1e-5, float(errm.max())
+    assert abs(float(kap) - kap_of(theta, masses)) <= 1e-11 * abs(float(kap))

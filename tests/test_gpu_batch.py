@@ -127,7 +127,7 @@ def test_batch_with_different_leads():
     it = b.items([om] + [w.omegas for w in other], "lpt")
     r = b.solve(it, "f64")
     P = om.size * len(pr.kpoints)
-    ref = pr.transmission(theta).reshape(-1)
+    ref = pr.transmission_theta(theta).reshape(-1)
     err = float(((r["T"][:P] - ref).abs() / ref.abs().clamp_min(1.0)).max())
     assert err <= TOL_T, err
 

@@ -50,19 +50,51 @@ def test_hermitian_and_psd():
         assert np.linalg.eigvalsh(d).min() > -1e-12
 
 
-def test_contract_is_the_derivative_of_a_linear_functional():
-    """For F(theta) = 2 Re sum Tr[D(theta) X] with fixed X, contract(X) = dF/dtheta."""
-    m = HeteroModel(seed=3, ny=2, nz_a=2, nz_b=3, n_layers=6, n_params=25)
+def test_block_gradient_convention():
+    """torch's gradient of F = 2 Re sum Tr[D X] with respect to complex D is
+    2 conj(X^T): the form the adjoint's backward returns."""
+    from negfpy_b200.adjoint import block_grads
+
     rng = np.random.default_rng(0)
+    shape = (2, 3, 5, 5)
+    X = torch.as_tensor(rng.normal(size=shape) + 1j * rng.normal(size=shape))
+    Y = torch.as_tensor(rng.normal(size=shape) + 1j * rng.normal(size=shape))
+    D = torch.zeros(shape, dtype=torch.complex128, requires_grad=True)
+    C = torch.zeros(shape, dtype=torch.complex128, requires_grad=True)
+    F = 2 * (torch.einsum("klab,klba->", D, X) + torch.einsum("klab,klba->", C, Y)).real
+    gD, gC = torch.autograd.grad(F, [D, C])
+    eD, eC = block_grads(X, Y)
+    assert torch.allclose(gD, eD, rtol=0, atol=1e-14) and torch.allclose(gC, eC, rtol=0, atol=1e-14)
+
+
+def test_blocks_are_differentiable_in_theta_and_masses():
+    """Autograd of a linear functional of the blocks against central differences."""
+    m = HeteroModel(seed=3, ny=2, nz_a=2, nz_b=3, n_layers=6, n_params=25)
+    rng = np.random.default_rng(1)
     K, L, n = len(KP), m.L, m.n
     xo = torch.as_tensor(rng.normal(size=(K, L, n, n)) + 1j * rng.normal(size=(K, L, n, n)))
     xc = torch.as_tensor(rng.normal(size=(K, L - 1, n, n)) + 1j * rng.normal(size=(K, L - 1, n, n)))
+
+    def F(th, ms):
+        on, cp = m.blocks(th, KP, ms)
+        return 2 * (torch.einsum("klab,klba->", on, xo) + torch.einsum("klab,klba->", cp, xc)).real
+
     th = torch.as_tensor(m.theta0, dtype=torch.float64).clone().requires_grad_(True)
-    on, cp = m.blocks(th, KP)
-    f = 2 * (torch.einsum("klab,klba->", on, xo) + torch.einsum("klab,klba->", cp, xc)).real
-    (g_ref,) = torch.autograd.grad(f, th)
-    g = m.contract(xo, xc, KP)
-    np.testing.assert_allclose(g.numpy(), g_ref.numpy(), rtol=1e-12, atol=1e-12 * float(g_ref.abs().max()))
+    ms = torch.as_tensor(m.mass, dtype=torch.float64).clone().requires_grad_(True)
+    g_th, g_m = torch.autograd.grad(F(th, ms), [th, ms])
+    h = 1e-6
+    for p in (0, 7, 24):
+        tp, tm = th.detach().clone(), th.detach().clone()
+        tp[p] += h
+        tm[p] -= h
+        fd = float(F(tp, ms.detach()) - F(tm, ms.detach())) / (2 * h)
+        assert abs(fd - float(g_th[p])) <= 1e-6 * max(1.0, abs(fd))
+    for q in (0, 5, 13, ms.numel() - 1):  # active and padding sites
+        mp, mm = ms.detach().clone().reshape(-1), ms.detach().clone().reshape(-1)
+        mp[q] += h
+        mm[q] -= h
+        fd = float(F(th.detach(), mp.reshape(ms.shape)) - F(th.detach(), mm.reshape(ms.shape))) / (2 * h)
+        assert abs(fd - float(g_m.reshape(-1)[q])) <= 1e-6 * max(1.0, abs(fd))
 
 
 def test_kappa_weights_trapezoid():
