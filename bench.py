@@ -211,7 +211,12 @@ def refined_vs_f64(torch, omega_stride=16):
     w = kappa_weights(om_w, 300.0, wl.omega_unit_rad_s)
     kap = {p: float((w * res[p]["T"].reshape(len(wi), K).mean(1)).sum()) for p in res}
     t64, tr = res["f64"]["T"], res["refined"]["T"]
+    tb64 = t64.reshape(len(wi), K).mean(1)
+    tbr = tr.reshape(len(wi), K).mean(1)
+    per_w = ((tbr - tb64).abs() / tb64.abs().clamp_min(1.0)).cpu().numpy()
     return {"workload": f"bulk_n96_L40_K256, every {omega_stride}th of 4096 omegas ({P} points)",
+            "Tbar_err_per_omega": {"max": float(per_w.max()), "median": float(np.median(per_w)),
+                                   "p99": float(np.quantile(per_w, 0.99))},
             "f64_points_per_s": P / ms["f64"] * 1e3, "refined_points_per_s": P / ms["refined"] * 1e3,
             "speedup": ms["f64"] / ms["refined"], "kappa_rel_err": (kap["refined"] - kap["f64"]) / kap["f64"],
             "T_max_rel_err": float(((tr - t64).abs() / t64.abs().clamp_min(1.0)).max()),

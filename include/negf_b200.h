@@ -256,6 +256,36 @@ int negf_kavg_f64(const double* t, int n_omega, int n_k, double* t_mean, void* s
 int negf_kappa_f64(const double* omega, const double* t_mean, int n_omega, const double* temperatures, int n_temps,
                    double omega_unit_rad_s, double* kappa_out, void* stream);
 
+/*
+ * k moments of an omega-major [n_omega][n_k] transmission table:
+ * t_mean[w] = <T>_k, t2_mean[w] = <T^2>_k.  Replaces the per-omega moments
+ * of negfpy workflows/ifc_bulk.py:1690-1784 (full counting statistics).
+ */
+int negf_kmoments_f64(const double* t, int n_omega, int n_k, double* t_mean, double* t2_mean, void* stream);
+
+/*
+ * First and second cumulants of the heat current from transmission moments
+ * on a strictly increasing grid omega_rad_s (rad/s):
+ *   c_out[0] = C1 (J/s) = (1/2pi) trapz(<T> (A_L - A_R), w),
+ *   c_out[1] = C2 (J^2/s) = (1/2pi) trapz(<T> (B_L + B_R) + (<T> + <T^2>) (A_L - A_R)^2, w),
+ * A = kB T x/expm1(x), B = (kB T)^2 x^2 e^x / expm1(x)^2, x = hbar w/(kB T).
+ * Replaces negfpy core/fcs.py:48-150 (heat_current_cumulants_from_k_moments;
+ * with t2_mean = T^2 also heat_current_cumulants_from_spectrum).
+ */
+int negf_fcs_cumulants_f64(const double* omega_rad_s, const double* t_mean, const double* t2_mean, int n_omega,
+                           double temp_left, double temp_right, double* c_out, void* stream);
+
+/*
+ * Landauer heat current of n_spectra transmission rows t[b][n_omega] on one
+ * strictly increasing grid omega_rad_s (rad/s):
+ *   j[b] = (1/2pi) trapz((kB T_L phi(x_L) - kB T_R phi(x_R)) t[b], omega),
+ *   phi(x) = x / expm1(x), x = hbar omega / (kB T), in W.
+ * Replaces negfpy core/thermal_current.py:30-67 (heat_current_from_spectrum
+ * and _spectral_bose_weight).  Temperatures must be positive.
+ */
+int negf_heat_current_f64(const double* omega_rad_s, const double* t, int n_omega, int n_spectra, double temp_left,
+                          double temp_right, double* j_out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

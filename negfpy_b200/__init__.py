@@ -29,6 +29,13 @@ from .dos import (
     leads_surface_dos_spectrum,
 )
 from .spectrum import kappa_from_grid, thermal_conductance_from_spectrum, transmission_grid
+from .thermal_current import (
+    heat_current_1d,
+    heat_current_density_3d,
+    heat_current_from_spectrum,
+    heat_current_per_length_2d,
+    transverse_length_from_vector,
+)
 from .models import (
     ChainParams,
     MaterialKspaceParams,

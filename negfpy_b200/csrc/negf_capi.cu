@@ -365,6 +365,35 @@ int negf_rgf_adjoint_f64(int n_dev, int n_lead_l, int n_lead_r, int n_layers, in
   return 0;
 }
 
+int negf_kmoments_f64(const double* t, int n_omega, int n_k, double* t_mean, double* t2_mean, void* stream) {
+  if (n_omega < 0 || n_k <= 0 || !t || !t_mean || !t2_mean) return fail(NEGF_EINVAL, "negf_kmoments_f64: bad argument");
+  if (negf::kmoments_launch(t, n_omega, n_k, t_mean, t2_mean, as_stream(stream)) != 0)
+    return cuda_fail("negf_kmoments_f64");
+  return 0;
+}
+
+int negf_fcs_cumulants_f64(const double* omega_rad_s, const double* t_mean, const double* t2_mean, int n_omega,
+                           double temp_left, double temp_right, double* c_out, void* stream) {
+  if (n_omega < 2 || !omega_rad_s || !t_mean || !t2_mean || !c_out)
+    return fail(NEGF_EINVAL, "negf_fcs_cumulants_f64: bad argument");
+  if (!(temp_left > 0.0) || !(temp_right > 0.0))
+    return fail(NEGF_EINVAL, "negf_fcs_cumulants_f64: temperature must be positive in Kelvin");
+  if (negf::fcs_launch(omega_rad_s, t_mean, t2_mean, n_omega, temp_left, temp_right, c_out, as_stream(stream)) != 0)
+    return cuda_fail("negf_fcs_cumulants_f64");
+  return 0;
+}
+
+int negf_heat_current_f64(const double* omega_rad_s, const double* t, int n_omega, int n_spectra, double temp_left,
+                          double temp_right, double* j_out, void* stream) {
+  if (n_omega < 2 || n_spectra < 0 || !omega_rad_s || !t || !j_out)
+    return fail(NEGF_EINVAL, "negf_heat_current_f64: bad argument");
+  if (!(temp_left > 0.0) || !(temp_right > 0.0))
+    return fail(NEGF_EINVAL, "negf_heat_current_f64: temperatures must be positive in Kelvin");
+  if (negf::heat_current_launch(omega_rad_s, t, n_omega, n_spectra, temp_left, temp_right, j_out, as_stream(stream)) != 0)
+    return cuda_fail("negf_heat_current_f64");
+  return 0;
+}
+
 int negf_kavg_f64(const double* t, int n_omega, int n_k, double* t_mean, void* stream) {
   if (n_omega < 0 || n_k <= 0 || !t || !t_mean) return fail(NEGF_EINVAL, "negf_kavg_f64: bad argument");
   if (negf::kavg_launch(t, n_omega, n_k, t_mean, as_stream(stream)) != 0) return cuda_fail("negf_kavg_f64");

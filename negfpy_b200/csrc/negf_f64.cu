@@ -965,6 +965,77 @@ __global__ void kavg_kernel(const double* __restrict__ T, int W, int K, double* 
   if (lane == 0) tbar[w] = s / (double)K;
 }
 
+// k moments <T> and <T^2> of an omega-major [W][K] table, one warp per omega
+// (the moments of negfpy workflows/ifc_bulk.py:1690-1784).
+__global__ void kmoments_kernel(const double* __restrict__ T, int W, int K, double* __restrict__ t1,
+                                double* __restrict__ t2) {
+  const int w = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (w >= W) return;
+  double s = 0.0, q = 0.0;
+  for (int k = lane; k < K; k += 32) {
+    const double v = T[(long long)w * K + k];
+    s += v;
+    q += v * v;
+  }
+  s = warp_sum(s);
+  q = warp_sum(q);
+  if (lane == 0) {
+    t1[w] = s / (double)K;
+    t2[w] = q / (double)K;
+  }
+}
+
+// Heat-current cumulants from transmission moments (negfpy
+// core/fcs.py:48-150), one block:
+//   C1 = (1/2pi) trapz(<T> (A_L - A_R), w),
+//   C2 = (1/2pi) trapz(<T> (B_L + B_R) + (<T> + <T^2>) (A_L - A_R)^2, w),
+//   A = kB T phi1(x), B = (kB T)^2 phi2(x), x = hbar w / (kB T),
+//   phi1 = x / expm1(x), phi2 = x^2 e^x / expm1(x)^2, with negfpy's series for
+//   |x| < 1e-6 and 0 from x = 700 on.
+__device__ __forceinline__ double fcs_phi1(double x) {
+  if (fabs(x) < 1e-6) return 1.0 - 0.5 * x + (x * x) / 12.0 - (x * x * x * x) / 720.0;
+  if (x < 700.0) return x / expm1(x);
+  return 0.0;
+}
+__device__ __forceinline__ double fcs_phi2(double x) {
+  if (fabs(x) < 1e-6) return 1.0 - (x * x) / 12.0 + (x * x * x * x) / 240.0;
+  if (x < 700.0) {
+    const double em1 = expm1(x);
+    return (x * x) * (em1 + 1.0) / (em1 * em1);
+  }
+  return 0.0;
+}
+__global__ void fcs_kernel(const double* __restrict__ om, const double* __restrict__ t1, const double* __restrict__ t2,
+                           int W, double temp_l, double temp_r, double* __restrict__ out) {
+  __shared__ double red[40];
+  const double hbar = 1.054571817e-34, kb = 1.380649e-23;
+  const double sl = kb * temp_l, sr = kb * temp_r;
+  double c1 = 0.0, c2 = 0.0;
+  for (int i = threadIdx.x; i < W - 1; i += blockDim.x) {
+    double f1[2], f2[2];
+    for (int q = 0; q < 2; ++q) {
+      const double w = om[i + q];
+      const double xl = hbar * w / sl, xr = hbar * w / sr;
+      const double ad = __dmul_rn(sl, fcs_phi1(xl)) - __dmul_rn(sr, fcs_phi1(xr));
+      const double bs = sl * sl * fcs_phi2(xl) + sr * sr * fcs_phi2(xr);
+      const double a = t1[i + q], b = t2[i + q];
+      f1[q] = a * ad;
+      f2[q] = a * bs + (a + b) * (ad * ad);
+    }
+    const double dw = om[i + 1] - om[i];
+    c1 += dw * (f1[0] + f1[1]) / 2.0;
+    c2 += dw * (f2[0] + f2[1]) / 2.0;
+  }
+  c1 = block_sum(c1, red);
+  c2 = block_sum(c2, red);
+  if (threadIdx.x == 0) {
+    const double pref = 1.0 / (2.0 * 3.141592653589793238462643383279502884);
+    out[0] = pref * c1;
+    out[1] = pref * c2;
+  }
+}
+
 // kappa(T) = (1/2pi) trapz(kB tbar(w) x^2 e^-x / (1 - e^-x)^2, w_rad), one
 // block per temperature (negfpy workflows/ifc_bulk.py:408-438).
 __global__ void kappa_kernel(const double* __restrict__ om, const double* __restrict__ tbar, int W,
@@ -993,6 +1064,37 @@ __global__ void kappa_kernel(const double* __restrict__ om, const double* __rest
   }
   s = block_sum(s, red);
   if (threadIdx.x == 0) out[blockIdx.x] = (temp > 0.0) ? (1.0 / (2.0 * 3.141592653589793238462643383279502884)) * s : 0.0;
+}
+
+// Landauer heat current of each spectrum row b (block b):
+//   J_b = (1/2pi) trapz((kB T_L phi(x_L) - kB T_R phi(x_R)) t_b(w), w),
+//   phi(x) = x / expm1(x), x = hbar w / (kB T), with the series
+//   1 - x/2 + x^2/12 below 1e-6 and 0 from 700 on (negfpy
+//   core/thermal_current.py:30-67).
+__device__ __forceinline__ double bose_phi(double x) {
+  if (x < 1e-6) return 1.0 - 0.5 * x + (x * x) / 12.0;
+  if (x < 700.0) return x / expm1(x);
+  return 0.0;
+}
+__global__ void heat_current_kernel(const double* __restrict__ om, const double* __restrict__ t, int W, double temp_l,
+                                    double temp_r, double* __restrict__ out) {
+  __shared__ double red[40];
+  const double hbar = 1.054571817e-34, kb = 1.380649e-23;
+  const double* row = t + (long long)blockIdx.x * W;
+  double s = 0.0;
+  for (int i = threadIdx.x; i < W - 1; i += blockDim.x) {
+    double f[2];
+    for (int q = 0; q < 2; ++q) {
+      const double w = om[i + q];
+      // separately rounded products: equal temperatures cancel exactly
+      const double wl = __dmul_rn(kb * temp_l, bose_phi(hbar * w / (kb * temp_l)));
+      const double wr = __dmul_rn(kb * temp_r, bose_phi(hbar * w / (kb * temp_r)));
+      f[q] = (wl - wr) * row[i + q];
+    }
+    s += (om[i + 1] - om[i]) * (f[0] + f[1]) / 2.0;
+  }
+  s = block_sum(s, red);
+  if (threadIdx.x == 0) out[blockIdx.x] = (1.0 / (2.0 * 3.141592653589793238462643383279502884)) * s;
 }
 
 // ---------------------------------------------------------------- launchers --
@@ -1112,6 +1214,26 @@ int kavg_launch(const double* T, int W, int K, double* tbar, cudaStream_t st) {
   if (W <= 0) return 0;
   const int wpb = 8;
   kavg_kernel<<<(W + wpb - 1) / wpb, wpb * 32, 0, st>>>(T, W, K, tbar);
+  return cudaGetLastError() == cudaSuccess ? 0 : -3;
+}
+
+int kmoments_launch(const double* T, int W, int K, double* t1, double* t2, cudaStream_t st) {
+  if (W <= 0) return 0;
+  const int wpb = 8;
+  kmoments_kernel<<<(W + wpb - 1) / wpb, wpb * 32, 0, st>>>(T, W, K, t1, t2);
+  return cudaGetLastError() == cudaSuccess ? 0 : -3;
+}
+
+int fcs_launch(const double* om, const double* t1, const double* t2, int W, double temp_l, double temp_r, double* out,
+               cudaStream_t st) {
+  fcs_kernel<<<1, 256, 0, st>>>(om, t1, t2, W, temp_l, temp_r, out);
+  return cudaGetLastError() == cudaSuccess ? 0 : -3;
+}
+
+int heat_current_launch(const double* om, const double* t, int W, int n_spectra, double temp_l, double temp_r,
+                        double* out, cudaStream_t st) {
+  if (n_spectra <= 0) return 0;
+  heat_current_kernel<<<n_spectra, 256, 0, st>>>(om, t, W, temp_l, temp_r, out);
   return cudaGetLastError() == cudaSuccess ? 0 : -3;
 }
 

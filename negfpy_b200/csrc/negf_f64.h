@@ -85,6 +85,11 @@ size_t grad_ws_bytes(int np, int n, int L, int grid);
 int grad_grid(int np);
 int grad_f64_launch(const GradArgs& ga, int np, int grid, double2* ws, cudaStream_t st);
 
+int heat_current_launch(const double* om, const double* t, int W, int n_spectra, double temp_l, double temp_r,
+                        double* out, cudaStream_t st);
+int kmoments_launch(const double* T, int W, int K, double* t1, double* t2, cudaStream_t st);
+int fcs_launch(const double* om, const double* t1, const double* t2, int W, double temp_l, double temp_r, double* out,
+               cudaStream_t st);
 int kavg_launch(const double* T, int W, int K, double* tbar, cudaStream_t st);
 int kappa_launch(const double* om, const double* tbar, int W, const double* temps, int nT, double unit, double* out,
                  cudaStream_t st);

@@ -278,3 +278,57 @@ def transmission_points(wl, pairs, processes=1, pool=None):
         if own:
             pool.close()
             pool.join()
+
+
+def heat_current_from_spectrum(omegas, tvals, temp_left, temp_right):
+    """Landauer heat current (W), ``core/thermal_current.py:30-67``: the
+    spectral Bose weight kB T_L phi(x_L) - kB T_R phi(x_R), phi(x) = x/expm1(x)
+    (series 1 - x/2 + x^2/12 below 1e-6, 0 from 700 on), trapezoid over omega
+    in rad/s, divided by 2 pi."""
+    hbar, kb = 1.054_571_817e-34, 1.380_649e-23
+    om = np.asarray(omegas, dtype=float)
+
+    def phi(x):
+        out = np.zeros_like(x)
+        small = x < 1e-6
+        mid = (x >= 1e-6) & (x < 700.0)
+        out[small] = 1.0 - 0.5 * x[small] + x[small] ** 2 / 12.0
+        out[mid] = x[mid] / np.expm1(x[mid])
+        return out
+
+    w = kb * temp_left * phi(hbar * om / (kb * temp_left)) - kb * temp_right * phi(hbar * om / (kb * temp_right))
+    f = w * np.asarray(tvals, dtype=float)
+    return float(np.sum(np.diff(om) * (f[1:] + f[:-1]) / 2.0) / (2.0 * np.pi))
+
+
+def fcs_cumulants(omegas, t1, t2, temp_left, temp_right):
+    """(C1, C2) of the heat current, ``core/fcs.py:48-150``: A = kB T phi1(x),
+    B = (kB T)^2 phi2(x), phi1 = x/expm1(x) (series 1 - x/2 + x^2/12 - x^4/720
+    for |x| < 1e-6), phi2 = x^2 e^x/expm1(x)^2 (series 1 - x^2/12 + x^4/240),
+    both 0 from x = 700 on; C1 = trapz(t1 (A_L - A_R))/2pi,
+    C2 = trapz(t1 (B_L + B_R) + (t1 + t2) (A_L - A_R)^2)/2pi."""
+    hbar, kb = 1.054_571_817e-34, 1.380_649e-23
+    om = np.asarray(omegas, dtype=float)
+
+    def phi(x, which):
+        out = np.zeros_like(x)
+        small = np.abs(x) < 1e-6
+        mid = (np.abs(x) >= 1e-6) & (x < 700.0)
+        xs = x[small]
+        if which == 1:
+            out[small] = 1.0 - 0.5 * xs + xs * xs / 12.0 - xs ** 4 / 720.0
+            out[mid] = x[mid] / np.expm1(x[mid])
+        else:
+            out[small] = 1.0 - xs * xs / 12.0 + xs ** 4 / 240.0
+            e = np.expm1(x[mid])
+            out[mid] = x[mid] ** 2 * (e + 1.0) / (e * e)
+        return out
+
+    sl, sr = kb * temp_left, kb * temp_right
+    ad = sl * phi(hbar * om / sl, 1) - sr * phi(hbar * om / sr, 1)
+    bs = sl * sl * phi(hbar * om / sl, 2) + sr * sr * phi(hbar * om / sr, 2)
+    t1, t2 = np.asarray(t1, dtype=float), np.asarray(t2, dtype=float)
+    f1 = t1 * ad
+    f2 = t1 * bs + (t1 + t2) * ad * ad
+    trap = lambda f: float(np.sum(np.diff(om) * (f[1:] + f[:-1]) / 2.0))  # noqa: E731
+    return trap(f1) / (2.0 * np.pi), trap(f2) / (2.0 * np.pi)

@@ -27,11 +27,61 @@ OUT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 
+def thermal(out_dir: Path) -> None:
+    """thermal.npz: negfpy's heat currents (core/thermal_current.py) on chain and square-lattice spectra."""
+    import negfpy.core as R
+    from negfpy.models import ChainParams, SquareLatticeParams, device_perfect_chain, lead_blocks
+    from negfpy.models import square_lattice_device, square_lattice_lead
+
+    from negfpy_b200 import workloads as W
+
+    wl = W.chain_workload()
+    unit = wl.omega_unit_rad_s
+    p = ChainParams(1.0, 1.0)
+    lead = lead_blocks(p)
+    dev = device_perfect_chain(8, p)
+    t_chain = np.array([R.transmission(float(w), dev, lead, lead, eta=1e-8) for w in wl.omegas])
+    om_rad = wl.omegas * unit
+    pairs = np.array([[310.0, 290.0], [50.0, 40.0], [1000.0, 10.0], [300.0, 300.0]])
+    j_spec = np.array([R.heat_current_from_spectrum(om_rad, t_chain, a, b) for a, b in pairs])
+    # heat_current_1d: its omegas are passed to transmission as they are (model units) and also used as rad/s
+    om1 = np.linspace(0.05, 1.95, 48)
+    j1 = R.heat_current_1d(om1, device_perfect_chain(6, p), lead, lead, 1e-10, 0.5e-10, eta=1e-8)
+    sq = SquareLatticeParams(mass=1.0, spring_x=1.0, spring_y=0.5)
+    kp = [(-np.pi / 2,), (0.0,), (np.pi / 3,)]
+    om2 = np.linspace(0.1, 2.2, 32)
+    j2 = R.heat_current_per_length_2d(om2, square_lattice_device(5, sq), square_lattice_lead(sq), square_lattice_lead(sq),
+                                      kp, 2.5, 2e-10, 1e-10, eta=1e-7)
+    j3 = R.heat_current_density_3d(om2, square_lattice_device(5, sq), square_lattice_lead(sq), square_lattice_lead(sq),
+                                   kp, 4.0, 2e-10, 1e-10, eta=1e-7)
+    tl = R.transverse_length_from_vector([1.0, 2.0, 0.5], [0.0, 1.0, 0.0])
+    # full counting statistics (core/fcs.py) on the chain spectrum and on k moments of the square lattice
+    from negfpy.core import fcs as F
+
+    c_spec = np.array([[F.heat_current_cumulants_from_spectrum(om_rad, t_chain, a, b).c1_j_per_s,
+                        F.heat_current_cumulants_from_spectrum(om_rad, t_chain, a, b).c2_j2_per_s] for a, b in pairs])
+    sqdev, sqlead = square_lattice_device(5, sq), square_lattice_lead(sq)
+    t_wk = np.array([[R.transmission(float(w), sqdev, sqlead, sqlead, eta=1e-7, kpar=k) for k in kp] for w in om2])
+    t1, t2 = t_wk.mean(axis=1), (t_wk ** 2).mean(axis=1)
+    om2_rad = om2 * unit
+    cm = F.heat_current_cumulants_from_k_moments(om2_rad, t1, t2, 300.0, 280.0)
+    unc = F.heat_current_uncertainty(cm, measurement_time_s=1e-6)
+    np.savez_compressed(out_dir / "thermal.npz", om_rad=om_rad, t_chain=t_chain, pairs=pairs, j_spec=j_spec,
+                        om1=om1, j1=j1, om2=om2, kp=np.array(kp), j2=j2, j3=j3, tl=tl, c_spec=c_spec,
+                        t_wk=t_wk, om2_rad=om2_rad, c_mom=np.array([cm.c1_j_per_s, cm.c2_j2_per_s]),
+                        unc=np.array([unc.std_current_j_per_s, unc.variance_energy_j2, unc.std_energy_j]))
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference/src")
+    ap.add_argument("--only", choices=["thermal"], default=None, help="write one fixture file only")
     args = ap.parse_args()
     sys.path.insert(0, args.ref)
+    if args.only == "thermal":
+        thermal(OUT)
+        print("wrote thermal.npz")
+        return
     import negfpy.core as R
     from negfpy.core.types import Device1D, LeadBlocks
     from negfpy.models import (ChainParams, MultiDofCellParams, SquareLatticeParams, device_perfect_chain,
@@ -144,6 +194,7 @@ def main() -> None:
                                              min_success_fraction=1.0)
     cases["chain_adaptive_T"] = np.array(tav)
     np.savez_compressed(OUT / "cases.npz", **cases)
+    thermal(OUT)
     print("wrote", sorted(p.name for p in OUT.glob("*.npz")))
 
 
