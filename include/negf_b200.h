@@ -128,6 +128,32 @@ int negf_rgf_transmission_f64_noalloc(int n_dev, int n_lead_l, int n_lead_r, int
                                       const int* k_index, const double* omega, const double* eta_device,
                                       const int* lead_status, double* t_out, int* status_out, void* stream);
 
+/* Workspace bytes negf_device_green_f64 needs (0 on a bad size). */
+size_t negf_device_green_workspace_bytes(int n_dev, int n_lead_l, int n_lead_r, int n_layers);
+
+/*
+ * Full device Green's function, FP64.  Replaces negfpy core/negf.py:253-303
+ * (device_green_function, there a dense SuperLU solve against the identity).
+ * Same inputs as negf_rgf_transmission_f64 with layer-resolved or shared
+ * blocks; per point p it writes
+ *   g_out[p]        G = A^-1, (n_layers n_dev)^2, row-major, every block,
+ *   sigma_l_out[p]  Sigma_L = V_L g_L V_L^H (n_dev x n_dev, first layer),
+ *   sigma_r_out[p]  Sigma_R (n_dev x n_dev, last layer),
+ *   status_out[p]   NEGF_* code (g_out is not written for failed points).
+ * One left sweep; the diagonal blocks by G_ii = g_i + g_i C_i G_{i+1,i+1}
+ * C_i^H g_i and the off-diagonal ones by G_ij = g_i C_i G_{i+1,j},
+ * G_ji = G_{j,i+1} C_i^H g_i (i < j).
+ */
+int negf_device_green_f64(int n_dev, int n_lead_l, int n_lead_r, int n_layers, int batch, const double* onsite,
+                          long long onsite_kstride, long long onsite_lstride, const double* coupling,
+                          long long coupling_kstride, long long coupling_lstride, const double* v_left,
+                          long long v_left_kstride, const double* v_right, long long v_right_kstride,
+                          const double* g_left, long long g_left_pstride, const double* g_right,
+                          long long g_right_pstride, const int* k_index, const double* omega,
+                          const double* eta_device, const int* lead_status, double* g_out, double* sigma_l_out,
+                          double* sigma_r_out, int* status_out, void* workspace, size_t workspace_bytes,
+                          void* stream);
+
 /* Workspace bytes negf_rgf_transmission_mixed needs (0 on a bad size). */
 size_t negf_rgf_mixed_workspace_bytes(int n_dev, int n_lead_l, int n_lead_r);
 

@@ -56,6 +56,12 @@ _SIGNATURES = {
     "negf_batch_transmission": (
         _I, [_P, _I, _I, _P, _P, _P, _I, _D, _I, _I, _I, _I, _P, _P, _P, _P, _SZ, _P],
     ),
+    "negf_device_green_workspace_bytes": (_SZ, [_I, _I, _I, _I]),
+    "negf_device_green_f64": (
+        _I,
+        [_I, _I, _I, _I, _I, _P, _LL, _LL, _P, _LL, _LL, _P, _LL, _P, _LL, _P, _LL, _P, _LL, _P, _P, _P, _P, _P,
+         _P, _P, _P, _P, _SZ, _P],
+    ),
     "negf_adjoint_workspace_bytes": (_SZ, [_I, _I, _I, _I]),
     "negf_rgf_adjoint_f64": (
         _I,

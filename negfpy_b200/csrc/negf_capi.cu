@@ -289,6 +289,82 @@ int negf_batch_transmission(const NegfBatchSystem* systems, int n_systems, int m
   return 0;
 }
 
+size_t negf_device_green_workspace_bytes(int n_dev, int n_lead_l, int n_lead_r, int n_layers) {
+  if (n_dev <= 0 || n_lead_l <= 0 || n_lead_r <= 0 || n_layers <= 0) return 0;
+  const int nmax = max3(n_dev, n_lead_l, n_lead_r);
+  if (nmax > 256) return 0;
+  const int np = (nmax + 15) / 16 * 16;
+  const int grid = negf::full_grid(np);
+  if (grid <= 0) return 0;
+  return kCounterBytes + negf::full_ws_bytes(np, n_dev, n_layers, grid);
+}
+
+int negf_device_green_f64(int n_dev, int n_lead_l, int n_lead_r, int n_layers, int batch, const double* onsite,
+                          long long onsite_kstride, long long onsite_lstride, const double* coupling,
+                          long long coupling_kstride, long long coupling_lstride, const double* v_left,
+                          long long v_left_kstride, const double* v_right, long long v_right_kstride,
+                          const double* g_left, long long g_left_pstride, const double* g_right,
+                          long long g_right_pstride, const int* k_index, const double* omega,
+                          const double* eta_device, const int* lead_status, double* g_out, double* sigma_l_out,
+                          double* sigma_r_out, int* status_out, void* workspace, size_t workspace_bytes,
+                          void* stream) {
+  if (n_dev <= 0 || n_lead_l <= 0 || n_lead_r <= 0 || n_layers <= 0 || batch < 0)
+    return fail(NEGF_EINVAL, "negf_device_green_f64: sizes must be positive");
+  if (!onsite || !v_left || !v_right || !g_left || !g_right || !omega || !eta_device || !g_out || !sigma_l_out ||
+      !sigma_r_out || (n_layers > 1 && !coupling))
+    return fail(NEGF_EINVAL, "negf_device_green_f64: null pointer");
+  if (onsite_kstride < 0 || onsite_lstride < 0 || coupling_kstride < 0 || coupling_lstride < 0 ||
+      v_left_kstride < 0 || v_right_kstride < 0 || g_left_pstride < 0 || g_right_pstride < 0)
+    return fail(NEGF_EINVAL, "negf_device_green_f64: negative stride");
+  const int nmax = max3(n_dev, n_lead_l, n_lead_r);
+  if (nmax > 256) return fail(NEGF_EUNSUPPORTED, "negf_device_green_f64: block order above 256");
+  const int np = (nmax + 15) / 16 * 16;
+  const int grid = negf::full_grid(np);
+  if (grid <= 0) return cuda_fail("negf_device_green_f64: occupancy query");
+  if (!workspace || workspace_bytes < kCounterBytes + negf::full_ws_bytes(np, n_dev, n_layers, grid))
+    return fail(NEGF_EINVAL, "negf_device_green_f64: workspace missing or too small");
+  if (batch == 0) return 0;
+  negf::FullArgs fa;
+  negf::RgfArgs& a = fa.r;
+  a.n = n_dev;
+  a.nl = n_lead_l;
+  a.nr = n_lead_r;
+  a.L = n_layers;
+  a.batch = batch;
+  a.D = reinterpret_cast<const double2*>(onsite);
+  a.d_ks = onsite_kstride;
+  a.d_ls = onsite_lstride;
+  a.C = reinterpret_cast<const double2*>(coupling ? coupling : onsite);
+  a.c_ks = coupling_kstride;
+  a.c_ls = coupling_lstride;
+  a.VL = reinterpret_cast<const double2*>(v_left);
+  a.vl_ks = v_left_kstride;
+  a.VR = reinterpret_cast<const double2*>(v_right);
+  a.vr_ks = v_right_kstride;
+  a.gL = reinterpret_cast<const double2*>(g_left);
+  a.gl_ps = g_left_pstride;
+  a.gR = reinterpret_cast<const double2*>(g_right);
+  a.gr_ps = g_right_pstride;
+  a.kidx = k_index;
+  a.omega = omega;
+  a.eta_dev = eta_device;
+  a.lead_status = lead_status;
+  a.T_out = nullptr;
+  a.status_out = status_out;
+  a.counter = reinterpret_cast<unsigned int*>(workspace);
+  a.sigma_ws = nullptr;
+  fa.G = reinterpret_cast<double2*>(g_out);
+  fa.sigL_out = reinterpret_cast<double2*>(sigma_l_out);
+  fa.sigR_out = reinterpret_cast<double2*>(sigma_r_out);
+  cudaStream_t st = as_stream(stream);
+  if (cudaMemsetAsync(workspace, 0, sizeof(unsigned int), st) != cudaSuccess)
+    return cuda_fail("negf_device_green_f64: counter reset");
+  if (negf::full_f64_launch(fa, np, grid, reinterpret_cast<double2*>(static_cast<char*>(workspace) + kCounterBytes),
+                            st) != 0)
+    return cuda_fail("negf_device_green_f64");
+  return 0;
+}
+
 size_t negf_adjoint_workspace_bytes(int n_dev, int n_lead_l, int n_lead_r, int n_layers) {
   if (n_dev <= 0 || n_lead_l <= 0 || n_lead_r <= 0 || n_layers <= 0) return 0;
   const int nmax = max3(n_dev, n_lead_l, n_lead_r);

@@ -53,6 +53,14 @@ struct GradArgs {
   double2* grad_c;       // [K][L-1][n][n]  += weight (X_{i+1,i} + X_{i,i+1}^H)
 };
 
+// Full device Green's function: RgfArgs plus the outputs.
+struct FullArgs {
+  RgfArgs r;
+  double2* G;         // [batch][L n][L n]
+  double2* sigL_out;  // [batch][n][n]
+  double2* sigR_out;  // [batch][n][n]
+};
+
 int padded_order(int n);
 const char* last_launch_error();  // message of the last failed launch on this thread
 int sr_f64_launch(const SrArgs& a, cudaStream_t st);
@@ -80,6 +88,10 @@ size_t batch_ws_bytes(int npmax, int grid);
 int batch_launch(const ::NegfBatchSystem* sys, int n_systems, const int* item_system, const int* item_k,
                  const double* item_omega, int n_items, double tol, int maxiter, double* t_out, int* status_out,
                  int* iters_out, int npmax, int mixed, int minb, int grid, void* counter, void* ws, cudaStream_t st);
+
+size_t full_ws_bytes(int np, int n, int L, int grid);
+int full_grid(int np);
+int full_f64_launch(const FullArgs& fa, int np, int grid, double2* ws, cudaStream_t st);
 
 size_t grad_ws_bytes(int np, int n, int L, int grid);
 int grad_grid(int np);

@@ -381,6 +381,123 @@ __global__ void __launch_bounds__(kThreads, 2) rgf_grad_f64_kernel(GradArgs ga, 
   }
 }
 
+// ------------------------------------------------------------ full device G --
+// Every block of G = A^-1 for one point (negfpy core/negf.py:253-303 builds it
+// densely with SuperLU).  One left sweep keeps g^L_i, W_i = g^L_i C_i and
+// V_i = C_i^H g^L_i; the diagonal follows backwards without further inverses,
+//   G_{L-1,L-1} = g^L_{L-1},  G_ii = g^L_i + W_i G_{i+1,i+1} V_i,
+// and the off-diagonal blocks by walking each column up and each row left,
+//   G_ij = W_i G_{i+1,j},  G_ji = G_{j,i+1} V_i   (i < j).
+// Blocks are written into G_out[p] (row-major, order L n); Sigma_L and Sigma_R
+// (n x n) into their outputs.
+__device__ void put_block(double2* Gp, long long dim, int bi, int bj, const double2* src, int n, int NP) {
+  for (int e = threadIdx.x; e < n * n; e += kThreads) {
+    const int r = e / n, c = e - r * n;
+    Gp[((long long)bi * n + r) * dim + (long long)bj * n + c] = src[(long long)r * NP + c];
+  }
+}
+
+__global__ void __launch_bounds__(kThreads, 2) rgf_full_f64_kernel(FullArgs fa, int NP, double2* ws) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const GJS sh = carve(smraw, NP);
+  __shared__ int s_point;
+  const RgfArgs& a = fa.r;
+  const int n = a.n, L = a.L, tid = threadIdx.x;
+  const int kch = (n + 7) >> 3;
+  const long long M2 = (long long)NP * NP;
+  const long long dim = (long long)L * n;
+  double2* base = ws + (long long)blockIdx.x * ((6 + 3LL * L) * M2 + 2LL * n * n);
+  double2 *Cb = base, *B1 = base + M2, *B2 = base + 2 * M2, *Xs = base + 3 * M2, *P0 = base + 4 * M2,
+          *P1 = base + 5 * M2;
+  double2* gl = base + 6 * M2;              // L slots: g^L_i, then G_ii
+  double2* Ws = gl + (long long)L * M2;     // L slots: W_i
+  double2* Vs = Ws + (long long)L * M2;     // L slots: V_i
+  double2* sigL = Vs + (long long)L * M2;
+  double2* sigR = sigL + (long long)n * n;
+
+  for (;;) {
+    if (tid == 0) s_point = (int)atomicAdd(a.counter, 1u);
+    __syncthreads();
+    const int p = s_point;
+    __syncthreads();
+    if (p >= a.batch) break;
+    const int lst = a.lead_status ? a.lead_status[p] : 0;
+    if (lst != kOk) {
+      if (tid == 0 && a.status_out) a.status_out[p] = lst;
+      continue;
+    }
+    const long long k = a.kidx ? (long long)a.kidx[p] : 0;
+    RgfPoint q;
+    q.n = n;
+    q.nl = a.nl;
+    q.nr = a.nr;
+    q.L = L;
+    q.D = a.D + k * a.d_ks;
+    q.d_ls = a.d_ls;
+    q.C = a.C + k * a.c_ks;
+    q.c_ls = a.c_ls;
+    q.VL = a.VL + k * a.vl_ks;
+    q.VR = a.VR + k * a.vr_ks;
+    q.gL = a.gL + (long long)p * a.gl_ps;
+    q.gR = a.gR + (long long)p * a.gr_ps;
+    q.z = z_of(a.omega[p], a.eta_dev[p]);
+    self_energies(q, NP, B1, B2, Xs, sigL, sigR);
+    for (int e = tid; e < n * n; e += kThreads) {
+      fa.sigL_out[(long long)p * n * n + e] = sigL[e];
+      fa.sigR_out[(long long)p * n * n + e] = sigR[e];
+    }
+    auto Dl = [&](int l) { return q.D + (long long)l * q.d_ls; };
+    int status = kOk;
+    // left sweep with W_l, V_l
+    form_m<false, false>(gl, nullptr, nullptr, Dl(0), sigL, L == 1 ? sigR : nullptr, q.z, n, NP, kch);
+    status = invert_into(gl, Xs, n, NP, sh);
+    for (int l = 1; l < L && status == kOk; ++l) {
+      load_pad(Cb, q.C + (long long)(l - 1) * q.c_ls, n, n, NP, 0.0);
+      __syncthreads();
+      gemm_to<false, false>(Ws + (l - 1) * M2, gl + (l - 1) * M2, Cb, NP, kch);
+      gemm_to<true, false>(Vs + (l - 1) * M2, Cb, gl + (l - 1) * M2, NP, kch);
+      form_m<true, false>(gl + l * M2, Cb, Ws + (l - 1) * M2, Dl(l), l == L - 1 ? sigR : nullptr, nullptr, q.z, n,
+                          NP, kch);
+      status = invert_into(gl + l * M2, Xs, n, NP, sh);
+    }
+    if (status == kOk) {
+      double2* Gp = fa.G + (long long)p * dim * dim;
+      // diagonal, backwards: G_ii = g^L_i + W_i G_{i+1,i+1} V_i (into the g^L slot)
+      put_block(Gp, dim, L - 1, L - 1, gl + (L - 1) * M2, n, NP);
+      for (int i = L - 2; i >= 0; --i) {
+        gemm_to<false, false>(P0, Ws + i * M2, gl + (i + 1) * M2, NP, kch);
+        gemm_to<false, false>(P1, P0, Vs + i * M2, NP, kch);
+        double2* gi = gl + i * M2;
+        for (long long e = tid; e < M2; e += kThreads) gi[e] = cadd(gi[e], P1[e]);
+        __syncthreads();
+        put_block(Gp, dim, i, i, gi, n, NP);
+      }
+      // columns up and rows left from each diagonal block
+      for (int j = 1; j < L; ++j) {
+        const double2* src = gl + j * M2;
+        double2 *x = P0, *y = P1;
+        for (int i = j - 1; i >= 0; --i) {
+          gemm_to<false, false>(x, Ws + i * M2, src, NP, kch);   // G_ij = W_i G_{i+1,j}
+          put_block(Gp, dim, i, j, x, n, NP);
+          src = x;
+          x = (x == P0) ? B1 : P0;
+        }
+        src = gl + j * M2;
+        for (int i = j - 1; i >= 0; --i) {
+          gemm_to<false, false>(y, src, Vs + i * M2, NP, kch);   // G_ji = G_{j,i+1} V_i
+          put_block(Gp, dim, j, i, y, n, NP);
+          src = y;
+          y = (y == P1) ? B2 : P1;
+        }
+        __syncthreads();
+      }
+    }
+    __syncthreads();
+    if (tid == 0 && a.status_out) a.status_out[p] = status;
+    __syncthreads();
+  }
+}
+
 // ---------------------------------------------------------------- launchers --
 size_t smem_bytes(int np) { return ((gjs_bytes(np) + 15) / 16) * 16 + 40 * 8; }
 
@@ -417,6 +534,21 @@ int grad_grid(int np) {
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   return g > 2 * nsm ? 2 * nsm : g;  // two blocks per SM bound the 2L-slot workspace
+}
+size_t full_ws_bytes(int np, int n, int L, int grid) {
+  return (size_t)grid * ((6 + 3 * (size_t)L) * np * np + 2 * (size_t)n * n) * 16;
+}
+int full_grid(int np) {
+  const int g = glob::occupancy_grid(glob::rgf_full_f64_kernel, np);
+  int dev = 0, nsm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  return g > 2 * nsm ? 2 * nsm : g;
+}
+int full_f64_launch(const FullArgs& fa, int np, int grid, double2* ws, cudaStream_t st) {
+  if (fa.r.batch <= 0) return 0;
+  glob::rgf_full_f64_kernel<<<grid, glob::kThreads, glob::smem_bytes(np), st>>>(fa, np, ws);
+  return cudaGetLastError() == cudaSuccess ? 0 : -3;
 }
 int grad_f64_launch(const GradArgs& ga, int np, int grid, double2* ws, cudaStream_t st) {
   if (ga.r.batch <= 0) return 0;

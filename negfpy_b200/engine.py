@@ -152,6 +152,45 @@ def rgf_transmission_refined(onsite, coupling, n_layers, vl, vr, gl, gr, omega, 
     return T, st, nbad
 
 
+def device_green(onsite: torch.Tensor, coupling: torch.Tensor | None, n_layers: int, vl: torch.Tensor,
+                 vr: torch.Tensor, gl: torch.Tensor, gr: torch.Tensor, omega: torch.Tensor, eta_dev: torch.Tensor,
+                 k_index: torch.Tensor | None, lead_status: torch.Tensor | None, stream=None):
+    """Full device G ``[P, L n, L n]`` and Sigma_L, Sigma_R ``[P, n, n]`` with status
+    (``negf_device_green_f64``); blocks as in ``rgf_transmission``."""
+    lib = _lib.load()
+    dev = _dev()
+    K, Lo, n, _ = onsite.shape
+    nl, nr = int(vl.shape[-1]), int(vr.shape[-1])
+    P = int(omega.shape[0])
+    dim = int(n_layers) * n
+    G = torch.empty((P, dim, dim), dtype=CDT, device=dev)
+    sl = torch.empty((P, n, n), dtype=CDT, device=dev)
+    sr = torch.empty((P, n, n), dtype=CDT, device=dev)
+    st = torch.empty(P, dtype=torch.int32, device=dev)
+    if P == 0:
+        return G, sl, sr, st
+    on_ks = Lo * n * n if K > 1 else 0
+    on_ls = 0 if Lo == 1 else n * n
+    if coupling is None or n_layers == 1:
+        cp, cp_ks, cp_ls = None, 0, 0
+    else:
+        Kc, Lc = coupling.shape[0], coupling.shape[1]
+        cp, cp_ks, cp_ls = coupling, (Lc * n * n if Kc > 1 else 0), (0 if Lc == 1 else n * n)
+    need = int(lib.negf_device_green_workspace_bytes(n, nl, nr, int(n_layers)))
+    if need == 0:
+        raise RuntimeError(f"block order {max(n, nl, nr)} is not supported by the device Green's function kernel")
+    ws = _workspace(need, dev, "device_green")
+    if k_index is not None:
+        k_index = k_index.to(device=dev, dtype=torch.int32).contiguous()
+    rc = lib.negf_device_green_f64(
+        n, nl, nr, int(n_layers), P, _lib.ptr(onsite), on_ks, on_ls, _lib.ptr(cp), cp_ks, cp_ls, _lib.ptr(vl),
+        n * nl if vl.shape[0] > 1 else 0, _lib.ptr(vr), n * nr if vr.shape[0] > 1 else 0, _lib.ptr(gl), nl * nl,
+        _lib.ptr(gr), nr * nr, _lib.ptr(k_index), _lib.ptr(omega), _lib.ptr(eta_dev), _lib.ptr(lead_status),
+        _lib.ptr(G), _lib.ptr(sl), _lib.ptr(sr), _lib.ptr(st), _lib.ptr(ws), ws.numel(), _lib.stream_handle(stream))
+    _lib.check(rc, "negf_device_green_f64")
+    return G, sl, sr, st
+
+
 def rgf_adjoint(onsite: torch.Tensor, coupling: torch.Tensor, n_layers: int, vl: torch.Tensor, vr: torch.Tensor,
                 gl: torch.Tensor, gr: torch.Tensor, omega: torch.Tensor, eta_dev: torch.Tensor,
                 k_index: torch.Tensor, lead_status: torch.Tensor | None, weight: torch.Tensor,

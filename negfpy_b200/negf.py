@@ -401,7 +401,37 @@ def transmission_kavg_adaptive_global_eta(omega: float, device, lead_left, lead_
         f"(required success_fraction >= {min_success_fraction:.3f}).")
 
 
-def device_green_function(*_args, **_kwargs):
-    """negfpy ``core/negf.py:253-303`` (full dense G) is not on the batched GPU path."""
-    raise NotImplementedError("device_green_function (full dense device G) is not provided by the GPU path; "
-                              "transmission() and the batched APIs compute only the contact block of G.")
+def device_green_function(omega: float, device, lead_left, lead_right, eta: float = 1e-8,
+                          eta_device: float | None = None, kpar=None, device_to_lead_left=None,
+                          device_to_lead_right=None, contact_left_indices=None, contact_right_indices=None,
+                          surface_gf_method: str = "sancho_rubio", omega_scale: float | None = None):
+    """(G, Sigma_L, Sigma_R) of the finite device (negfpy ``core/negf.py:253-303``).
+
+    G is the dense (L n) x (L n) inverse of A = (omega + i eta_d)^2 - D - Sigma,
+    every block computed on the GPU by a left-connected sweep and backward
+    recursions (``negf_device_green_f64``); Sigma_L and Sigma_R are embedded in
+    (L n) x (L n) matrices at the contact indices, as negfpy returns them.  The
+    contacts must lie in the first / last principal layer (``ValueError``
+    otherwise, as for ``transmission``)."""
+    check_method(surface_gf_method)
+    dev = _lib.require_cuda()
+    s = point_system(omega, device, lead_left, lead_right, eta, eta_device, kpar, device_to_lead_left,
+                     device_to_lead_right, contact_left_indices, contact_right_indices, omega_scale)
+    sysobj, _ = stack_systems([s])
+    om = torch.tensor([s["omega"]], dtype=torch.float64, device=dev)
+    et = torch.tensor([s["eta"]], dtype=torch.float64, device=dev)
+    ed = torch.tensor([s["eta_dev"]], dtype=torch.float64, device=dev)
+    ki = torch.zeros(1, dtype=torch.int32, device=dev)
+    rl = engine.sgf_sr(*sysobj.lead_l, om, et, ki)
+    rr = rl if sysobj.same_leads else engine.sgf_sr(*sysobj.lead_r, om, et, ki)
+    lst = torch.where(rl["status"] != 0, rl["status"], rr["status"])
+    G, sl, sr, st = engine.device_green(sysobj.onsite, sysobj.coupling, sysobj.n_layers, sysobj.vl, sysobj.vr,
+                                        rl["g"], rr["g"], om, ed, ki, lst)
+    raise_for_status(int(st[0]))
+    n = sysobj.n
+    dim = sysobj.n_layers * n
+    sigma_l = np.zeros((dim, dim), dtype=np.complex128)
+    sigma_r = np.zeros((dim, dim), dtype=np.complex128)
+    sigma_l[:n, :n] = sl[0].cpu().numpy()
+    sigma_r[dim - n:, dim - n:] = sr[0].cpu().numpy()
+    return G[0].cpu().numpy(), sigma_l, sigma_r

@@ -332,3 +332,36 @@ def fcs_cumulants(omegas, t1, t2, temp_left, temp_right):
     f2 = t1 * bs + (t1 + t2) * ad * ad
     trap = lambda f: float(np.sum(np.diff(om) * (f[1:] + f[:-1]) / 2.0))  # noqa: E731
     return trap(f1) / (2.0 * np.pi), trap(f2) / (2.0 * np.pi)
+
+
+def device_green_point(omega, onsite, coupling, lead_l, lead_r, eta=1e-8, eta_device=None, vl=None, vr=None,
+                       idx_l=None, idx_r=None, tol=1e-12, maxiter=200):
+    """(G, Sigma_L, Sigma_R) of the finite device, ``core/negf.py:253-303``:
+    the system matrix of ``transmission_point``, G = A^-1 by SuperLU against
+    the identity, and the self-energies embedded at the contact indices."""
+    L = len(onsite)
+    n = onsite[0].shape[0]
+    dim = L * n
+    eta_dev = float(eta if eta_device is None else eta_device)
+    d00l, d01l, d10l = lead_l
+    d00r, d01r, d10r = lead_r
+    if vl is None:
+        vl = d10l if d10l is not None else np.conj(d01l).T
+    if vr is None:
+        vr = d01r
+    vl, vr = np.asarray(vl, dtype=np.complex128), np.asarray(vr, dtype=np.complex128)
+    il = np.arange(vl.shape[0]) if idx_l is None else np.asarray(idx_l, dtype=int).ravel()
+    ir = np.arange(dim - vr.shape[0], dim) if idx_r is None else np.asarray(idx_r, dtype=int).ravel()
+    gl, _ = sancho_rubio(omega, d00l, d01l, d10l, eta, tol, maxiter)
+    gr, _ = sancho_rubio(omega, d00r, d01r, d10r, eta, tol, maxiter)
+    sl, sr = self_energy(vl, gl), self_energy(vr, gr)
+    z = (omega + 1j * eta_dev) ** 2
+    a = (z * sparse.identity(dim, dtype=np.complex128, format="csc") - _assemble_device(onsite, coupling)).tolil()
+    a[np.ix_(il, il)] = a[np.ix_(il, il)] - sl
+    a[np.ix_(ir, ir)] = a[np.ix_(ir, ir)] - sr
+    g = splu(a.tocsc()).solve(np.eye(dim, dtype=np.complex128))
+    sig_l = np.zeros((dim, dim), dtype=np.complex128)
+    sig_r = np.zeros((dim, dim), dtype=np.complex128)
+    sig_l[np.ix_(il, il)] = sl
+    sig_r[np.ix_(ir, ir)] = sr
+    return g, sig_l, sig_r

@@ -72,15 +72,54 @@ def thermal(out_dir: Path) -> None:
                         unc=np.array([unc.std_current_j_per_s, unc.variance_energy_j2, unc.std_energy_j]))
 
 
+def green(out_dir: Path) -> None:
+    """green.npz: negfpy's device_green_function (core/negf.py:253-303) on small systems."""
+    import negfpy.core as R
+    from negfpy.core.types import Device1D, LeadBlocks
+    from negfpy.models import ChainParams, MultiDofCellParams, device_perfect_chain, lead_blocks
+    from negfpy.models import multidof_device, multidof_lead_blocks
+
+    from negfpy_b200 import workloads as W
+
+    out = {}
+    p = ChainParams(1.0, 1.0)
+    lead = lead_blocks(p)
+    out["chain_G"], out["chain_SL"], out["chain_SR"] = R.device_green_function(1.1, device_perfect_chain(6, p), lead,
+                                                                               lead, eta=1e-8)
+    lead1 = LeadBlocks(d00=np.array([[2.0]], dtype=np.complex128), d01=np.array([[-1.0]], dtype=np.complex128))
+    onsite = [np.diag([2.0, 100.0]).astype(np.complex128) for _ in range(4)]
+    coupling = [np.diag([-1.0, 0.0]).astype(np.complex128) for _ in range(3)]
+    out["rect_G"], out["rect_SL"], out["rect_SR"] = R.device_green_function(
+        1.0, Device1D(onsite, coupling), lead1, lead1, eta=1e-8, device_to_lead_left=np.array([[-1.0]]),
+        device_to_lead_right=np.array([[-1.0]]), contact_left_indices=[0], contact_right_indices=[6])
+    md = MultiDofCellParams(masses=np.ones(2), fc00=2.0 * np.eye(6), fc01=-np.eye(6), dof_per_atom=3)
+    out["md_G"], out["md_SL"], out["md_SR"] = R.device_green_function(0.7, multidof_device(5, md),
+                                                                      multidof_lead_blocks(md),
+                                                                      multidof_lead_blocks(md), eta=1e-7,
+                                                                      eta_device=2e-7)
+    wl = W.slab_workload()
+    ki = 13
+    lb = LeadBlocks(d00=wl.lead_l["d00"][ki], d01=wl.lead_l["d01"][ki], d10=wl.lead_l["d10"][ki])
+    dv = Device1D(onsite_blocks=[wl.onsite[ki, 0]] * 3, coupling_blocks=[wl.coupling[ki, 0]] * 2)
+    out["slab_G"], out["slab_SL"], out["slab_SR"] = R.device_green_function(float(wl.omegas[900]), dv, lb, lb,
+                                                                            eta=wl.eta, omega_scale=1.3)
+    out["slab_omega"], out["slab_eta"], out["slab_k"] = float(wl.omegas[900]), wl.eta, ki
+    np.savez_compressed(out_dir / "green.npz", **out)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference/src")
-    ap.add_argument("--only", choices=["thermal"], default=None, help="write one fixture file only")
+    ap.add_argument("--only", choices=["thermal", "green"], default=None, help="write one fixture file only")
     args = ap.parse_args()
     sys.path.insert(0, args.ref)
     if args.only == "thermal":
         thermal(OUT)
         print("wrote thermal.npz")
+        return
+    if args.only == "green":
+        green(OUT)
+        print("wrote green.npz")
         return
     import negfpy.core as R
     from negfpy.core.types import Device1D, LeadBlocks
@@ -195,6 +234,7 @@ def main() -> None:
     cases["chain_adaptive_T"] = np.array(tav)
     np.savez_compressed(OUT / "cases.npz", **cases)
     thermal(OUT)
+    green(OUT)
     print("wrote", sorted(p.name for p in OUT.glob("*.npz")))
 
 
