@@ -129,14 +129,19 @@ class HeteroKappaProblem(DeviceSolve):
     """kappa(theta, masses) of a ``HeteroModel`` between its leads A and B on an (omega x k) grid."""
 
     def __init__(self, model: HeteroModel, kpoints, omegas, eta: float, temperature: float = 300.0,
-                 omega_unit_rad_s: float = 1.0, tol: float = 1e-12, maxiter: int = 200):
+                 omega_unit_rad_s: float = 1.0, tol: float = 1e-12, maxiter: int = 200,
+                 w_kappa: torch.Tensor | None = None):
+        """``w_kappa``: kappa weights of these omegas when they are a shard of a
+        larger grid (default: the trapezoid over these omegas alone)."""
         self.model, self.kpoints = model, list(kpoints)
+        self.eta0, self.temperature, self.omega_unit_rad_s = float(eta), float(temperature), float(omega_unit_rad_s)
         la = model.lead_blocks("A", self.kpoints)
         lb = model.lead_blocks("B", self.kpoints)
         vl = np.zeros((len(self.kpoints), model.n, model.n_a), dtype=complex)
         vl[:, model.contact_left_indices(), :] = la["d10"]
         super().__init__(la, lb, vl, lb["d01"], model.L, omegas, len(self.kpoints), eta, tol, maxiter)
-        self.w_kappa = kappa_weights(self.om, temperature, omega_unit_rad_s)
+        self.w_kappa = (kappa_weights(self.om, temperature, omega_unit_rad_s) if w_kappa is None
+                        else torch.as_tensor(w_kappa, dtype=torch.float64, device=self.om.device))
 
     def blocks(self, theta: torch.Tensor, masses: torch.Tensor | None = None):
         return self.model.blocks(theta, self.kpoints, masses)

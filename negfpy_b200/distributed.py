@@ -63,3 +63,43 @@ def transmission_grid_sharded(omegas, kpoints, device, lead_left, lead_right, gr
     T = gather_rows(torch.as_tensor(res["T"], device=dev), om.size, group)
     st = gather_rows(torch.as_tensor(res["status"].astype(np.int32), device=dev), om.size, group)
     return {"T": T.cpu().numpy(), "status": st.cpu().numpy(), "shard": shard}
+
+
+def sharded_weighted_sum(local_fn, omegas, weights, group=None):
+    """sum_w weights[w] f(w) and its parameter gradients over the ranks.
+
+    Every rank evaluates ``local_fn(omegas[shard], weights[shard])`` ->
+    ``(value, *grads)`` (tensors) on its strided omega shard with the GLOBAL
+    weights restricted to it (a trapezoid weight depends on both
+    neighbours, so the shard must not re-derive them), then one all-reduce
+    (sum) per output combines the ranks.  All ranks must call it."""
+    om = np.asarray(omegas, dtype=float)
+    w = np.asarray(weights, dtype=float)
+    world = dist.get_world_size(group)
+    rank = dist.get_rank(group)
+    shard = omega_shard(om.size, rank, world)
+    outs = [torch.as_tensor(o).clone() for o in local_fn(om[shard], w[shard])]
+    for o in outs:
+        dist.all_reduce(o, op=dist.ReduceOp.SUM, group=group)
+    return tuple(outs)
+
+
+def hetero_kappa_grad_sharded(model, kpoints, omegas, eta, theta, masses=None, temperature=300.0,
+                              omega_unit_rad_s=1.0, group=None):
+    """kappa, dkappa/dtheta and dkappa/dmasses of a heterojunction with the
+    omega grid sharded over the ranks (one adjoint launch per rank, one
+    all-reduce of kappa and of each gradient: 2000 + 720 doubles for the
+    differentiation workload).  Each rank computes on its current CUDA device."""
+    from .adjoint import HeteroKappaProblem, kappa_weights
+
+    om = np.asarray(omegas, dtype=float)
+    w_all = kappa_weights(torch.as_tensor(om), temperature, omega_unit_rad_s).numpy()
+
+    def local(om_s, w_s):
+        pr = HeteroKappaProblem(model, kpoints, om_s, eta, temperature, omega_unit_rad_s,
+                                w_kappa=torch.as_tensor(w_s))
+        k, g_th, g_m = pr.kappa_and_grad(theta, masses)
+        return k.reshape(1), g_th, g_m
+
+    k, g_th, g_m = sharded_weighted_sum(local, om, w_all, group)
+    return k[0], g_th, g_m

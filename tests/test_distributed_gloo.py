@@ -70,3 +70,38 @@ def test_two_gloo_ranks_gather_the_serial_spectrum(tmp_path):
     k_full = O.thermal_conductance(omegas, full[:, 0], [300.0], unit)
     k_serial = O.thermal_conductance(omegas, serial[:, 0], [300.0], unit)
     assert np.array_equal(k_full, k_serial)
+
+
+def _grad_worker(rank, world, port, omegas, weights, out_dir):
+    """Fake local solve: value sum_w w f(w), gradient sum_w w df/dp, on CPU."""
+    from negfpy_b200.distributed import sharded_weighted_sum
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=__import__("datetime").timedelta(seconds=60))
+    try:
+        def local(om, w):
+            f = np.sin(om) ** 2
+            g = np.stack([np.cos(om) * w, om * w]).sum(axis=1)
+            return torch.tensor([float((w * f).sum())], dtype=torch.float64), torch.as_tensor(g)
+
+        k, g = sharded_weighted_sum(local, omegas, weights)
+        np.save(os.path.join(out_dir, f"kg_{rank}.npy"), np.concatenate([k.numpy(), g.numpy()]))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_reduce_kappa_and_gradient(tmp_path):
+    """The sharded weighted sum with global trapezoid weights equals the serial one."""
+    from negfpy_b200.adjoint import kappa_weights
+
+    omegas = (np.arange(17, dtype=float) + 1.0) * 0.11
+    weights = kappa_weights(torch.as_tensor(omegas), 300.0, 2 * np.pi * 15e12 / 2.0).numpy()
+    world = 2
+    mp.spawn(_grad_worker, args=(world, _free_port(), omegas, weights, str(tmp_path)), nprocs=world, join=True)
+    serial = np.concatenate([[float((weights * np.sin(omegas) ** 2).sum())],
+                             [float((np.cos(omegas) * weights).sum()), float((omegas * weights).sum())]])
+    for r in range(world):
+        got = np.load(tmp_path / f"kg_{r}.npy")
+        np.testing.assert_allclose(got, serial, rtol=1e-13, atol=0)

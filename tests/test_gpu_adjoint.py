@@ -174,3 +174,32 @@ def test_hetero_grads_match_central_differences(hetero):
     errm = np.abs(np.array(fdm) - gm[msel]) / np.abs(gm).max()
     assert float(errm.max()) < 1e-5, float(errm.max())
     assert abs(float(kap) - kap_of(theta, masses)) <= 1e-11 * abs(float(kap))
+
+
+def test_sharded_gradient_one_rank(hetero):
+    """The omega-sharded gradient path (all-reduce over ranks) on one NCCL rank
+    equals the unsharded one."""
+    import os
+    import socket
+
+    import torch.distributed as dist
+
+    from negfpy_b200.distributed import hetero_kappa_grad_sharded
+
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("nccl", rank=0, world_size=1, timeout=__import__("datetime").timedelta(seconds=60))
+    try:
+        m = hetero.model
+        theta = torch.as_tensor(m.theta0, device="cuda")
+        k, g_th, g_m = hetero_kappa_grad_sharded(m, hetero.kpoints, hetero.om.cpu().numpy(), hetero.eta0, theta,
+                                                 None, hetero.temperature, hetero.omega_unit_rad_s)
+        k0, g0, gm0 = hetero.kappa_and_grad(theta)
+        assert abs(float(k) - float(k0)) <= 1e-13 * abs(float(k0))
+        # the adjoint blocks are summed with FP64 atomics, in run-dependent order
+        assert _rel(g_th, g0) < 1e-11 and _rel(g_m, gm0) < 1e-11
+    finally:
+        dist.destroy_process_group()
