@@ -1,0 +1,325 @@
+"""The workflow's transmission stage as batched GPU work (negfpy
+``workflows/ifc_bulk.py:1059-1288``, ``_run_transmission``).
+
+negfpy runs one task per omega in a thread or process pool, and each task
+calls ``transmission_kavg_adaptive`` (per-k eta ladder), ``..._global_eta``
+(one eta per omega) or the global form with the fixed eta, over the low or
+the high k mesh of that omega.  Here the blocks of both meshes are uploaded
+once, and every ladder rung is ONE launch over all pending (omega, k) points
+of all omegas, each point with its own eta.  The acceptance tests, the
+statistics, the eta records, the failure records, the rejected lists and the
+post-processing of the values are negfpy's.
+
+The ``solver.parallel`` settings are parsed and reported as negfpy reports
+them; they do not change the execution (there is no pool).  The surface GF
+method must be Sancho-Rubio (``NotImplementedError`` otherwise; negfpy's
+workflow default is ``generalized_eigen_svd``, which is the oracle here).
+"""
+
+from __future__ import annotations
+
+import os
+from typing import Any
+
+import numpy as np
+import torch
+
+from . import _lib
+from .negf import _check_adaptive_args, _classify, _prepare_ladder_systems, stack_systems
+from .surface_gf import check_method
+
+# CODATA 2018 constants, as negfpy modeling/units.py:8-16.
+RYDBERG_J = 2.1798723611035e-18
+BOHR_M = 5.29177210903e-11
+ELECTRON_MASS_KG = 9.1093837015e-31
+QE_RY_MASS_UNIT_KG = 2.0 * ELECTRON_MASS_KG
+SPEED_OF_LIGHT_CM_S = 2.99792458e10
+HBAR_J_S = 1.054571817e-34
+EV_J = 1.602176634e-19
+
+DEFAULT_ETA_VALUES: tuple[float, ...] = (1e-8, 1e-7, 1e-6, 1e-5, 1e-4, 1e-3)  # workflows/ifc_bulk.py:54
+
+
+def qe_omega_to_rad_s(omega):
+    """QE-q2r internal omega -> rad/s (negfpy modeling/units.py:18-26)."""
+    return np.asarray(omega) * np.sqrt(RYDBERG_J / (QE_RY_MASS_UNIT_KG * BOHR_M * BOHR_M))
+
+
+def qe_omega_to_cm1(omega):
+    """QE-q2r internal omega -> cm^-1 (negfpy modeling/units.py:36-40)."""
+    return np.asarray(qe_omega_to_rad_s(omega), dtype=float) / (2.0 * np.pi * SPEED_OF_LIGHT_CM_S)
+
+
+def qe_ev_to_omega(ev):
+    """Phonon energy in eV -> QE-q2r internal omega (negfpy modeling/units.py:43-54)."""
+    factor = float(np.asarray(qe_omega_to_rad_s(1.0), dtype=float)) * HBAR_J_S / EV_J
+    return np.asarray(ev, dtype=float) / factor
+
+
+def resolve_eta_values_for_omega(omega: float, omega_cm1: float, *, eta_values: tuple[float, ...],
+                                 max_eta_over_omega: float | None, eta_ratio_cm1_min: float | None) -> tuple:
+    """negfpy ``workflows/ifc_bulk.py:581-595``."""
+    if max_eta_over_omega is None:
+        return eta_values
+    apply_cap = eta_ratio_cm1_min is None or omega_cm1 >= eta_ratio_cm1_min
+    if not apply_cap:
+        return eta_values
+    filtered = tuple(e for e in eta_values if (e / omega) <= max_eta_over_omega)
+    return filtered if len(filtered) > 0 else (min(eta_values),)
+
+
+def resolve_parallel_solver_config(scfg: dict[str, Any]) -> dict[str, Any]:
+    """negfpy ``workflows/ifc_bulk.py:598-617`` (reported, not used for execution)."""
+    pcfg = dict(scfg.get("parallel", {}))
+    enabled = bool(pcfg.get("enabled", False))
+    backend = str(pcfg.get("backend", "thread")).lower()
+    if backend not in {"thread", "process"}:
+        raise ValueError("solver.parallel.backend must be one of: thread, process.")
+    workers_raw = pcfg.get("workers", None)
+    workers = int(os.cpu_count() or 1) if workers_raw is None else int(workers_raw)
+    workers = max(workers, 1)
+    blas_threads_raw = pcfg.get("blas_threads", 1 if enabled else None)
+    blas_threads = None if blas_threads_raw is None else max(int(blas_threads_raw), 1)
+    return {"enabled": enabled and workers > 1, "backend": backend, "workers": workers, "blas_threads": blas_threads}
+
+
+class _Mesh:
+    """The device-resident blocks of one k mesh, and the per-k acceptance limits."""
+
+    def __init__(self, kpoints, device, lead_left, lead_right, eta_device, vdl_left, vdl_right, omega_scale,
+                 max_channel_factor):
+        self.kpoints = list(kpoints)
+        systems = _prepare_ladder_systems(1.0, device, lead_left, lead_right, self.kpoints, eta_device, vdl_left,
+                                          vdl_right, None, None, omega_scale)
+        self.sys, _ = stack_systems(systems)
+        self.scale = systems[0]["scale"]
+        self.eta_dev_for = systems[0]["_eta_dev_for"]
+        nl = int(self.sys.nl)
+        self.max_allowed = None if max_channel_factor is None else float(max_channel_factor) * float(nl)
+
+
+def _solve(mesh: _Mesh, omegas: list, etas: list, ks: list) -> tuple[np.ndarray, np.ndarray]:
+    """T and status of (omega, eta, k) points of one mesh in one launch."""
+    dev = _lib.require_cuda()
+    P = len(omegas)
+    if P == 0:
+        return np.zeros(0), np.zeros(0, dtype=np.int32)
+    eds = [mesh.eta_dev_for(e) for e in etas]
+    T = np.full(P, np.nan)
+    st = np.full(P, -1, dtype=np.int32)
+    ok = [i for i in range(P) if eds[i] >= 0.0]  # a negative device eta is negfpy's ValueError
+    if ok:
+        om = torch.tensor([omegas[i] / mesh.scale for i in ok], dtype=torch.float64, device=dev)
+        et = torch.tensor([etas[i] / mesh.scale for i in ok], dtype=torch.float64, device=dev)
+        ed = torch.tensor([eds[i] for i in ok], dtype=torch.float64, device=dev)
+        ki = torch.tensor([ks[i] for i in ok], dtype=torch.int32, device=dev)
+        r = mesh.sys.transmission(om, ki, et, ed)
+        T[ok] = r["T"].cpu().numpy()
+        st[ok] = r["status"].cpu().numpy()
+    return T, st
+
+
+def _rejected(omega, kp, eta, t, reason):
+    return {"omega": float(omega), "kpar": tuple(float(x) for x in kp) if kp is not None else (), "eta": float(eta),
+            "t": None if reason == "exception" else float(t), "reason": reason}
+
+
+def run_transmission(cfg: dict[str, Any], *, device, lead_left, lead_right, device_to_lead_left=None,
+                     device_to_lead_right=None, omegas: np.ndarray, kmesh: dict[str, Any]) -> dict[str, Any]:
+    """k-averaged T(omega) of the workflow with its eta scheme, batched on the GPU.
+
+    Same arguments, configuration keys and result dictionary as negfpy's
+    ``_run_transmission`` (``workflows/ifc_bulk.py:1059-1288``)."""
+    scfg = dict(cfg.get("solver", {}))
+    sgf_method = str(scfg.get("surface_gf_method", "generalized_eigen_svd"))
+    eta_scheme = str(scfg.get("eta_scheme", "adaptive")).lower().replace("-", "_")
+    eta_fixed = float(scfg.get("eta_fixed", 1e-4))
+    eta_values_base = tuple(float(v) for v in scfg.get("eta_values", DEFAULT_ETA_VALUES))
+    eta_device_raw = scfg.get("eta_device", None)
+    eta_device = None if eta_device_raw is None else float(eta_device_raw)
+    min_success_fraction = float(scfg.get("min_success_fraction", 0.7))
+    nonnegative_tolerance = float(scfg.get("nonnegative_tolerance", 1e-8))
+    max_channel_factor_raw = scfg.get("max_channel_factor", 1.5)
+    max_channel_factor = None if max_channel_factor_raw is None else float(max_channel_factor_raw)
+    collect_rejected = bool(scfg.get("collect_rejected", False))
+    max_eta_over_omega_raw = scfg.get("max_eta_over_omega", None)
+    max_eta_over_omega = None if max_eta_over_omega_raw is None else float(max_eta_over_omega_raw)
+    eta_ratio_cm1_min_raw = scfg.get("eta_ratio_cm1_min", None)
+    eta_ratio_cm1_min = None if eta_ratio_cm1_min_raw is None else float(eta_ratio_cm1_min_raw)
+    parallel_cfg = resolve_parallel_solver_config(scfg)
+    omega_scale_mode = str(scfg.get("omega_scale_mode", "none")).lower()
+    if omega_scale_mode == "ev":
+        omega_scale = float(np.asarray(qe_ev_to_omega(1.0), dtype=float))
+    elif omega_scale_mode == "none":
+        omega_scale = None
+    else:
+        raise ValueError("solver.omega_scale_mode must be 'none' or 'ev'.")
+    check_method(sgf_method)
+    per_k = eta_scheme not in ("fixed", "adaptive_global")
+
+    omegas = np.asarray(omegas, dtype=float)
+    W = omegas.size
+    vals = np.zeros(W, dtype=float)
+    results: list[dict | None] = [None] * W
+    meshes: dict[str, _Mesh] = {}
+    tasks = []  # (index, omega, omega_cm1, mesh name, eta ladder)
+    for i, w in enumerate(omegas):
+        w = float(w)
+        if w <= 0.0:
+            results[i] = {"value": 0.0, "eta_record": None, "failure": None}
+            continue
+        w_cm1 = float(np.asarray(qe_omega_to_cm1(w), dtype=float))
+        use_low = bool(w_cm1 <= float(kmesh["low_cm1"]))
+        name = "low" if use_low else "high"
+        ladder = resolve_eta_values_for_omega(w, w_cm1, eta_values=eta_values_base,
+                                              max_eta_over_omega=max_eta_over_omega,
+                                              eta_ratio_cm1_min=eta_ratio_cm1_min)
+        if eta_scheme == "fixed":
+            ladder = (eta_fixed,)
+        kpts = kmesh[name]["kpoints"]
+        try:
+            _check_adaptive_args(kpts, ladder, min_success_fraction, nonnegative_tolerance, max_channel_factor)
+        except Exception as exc:  # negfpy's task turns every exception into a failure record
+            results[i] = {"value": np.nan, "eta_record": None,
+                          "failure": {"omega_qe": w, "omega_cm1": w_cm1, "error": str(exc)}}
+            continue
+        if name not in meshes:
+            meshes[name] = _Mesh(kpts, device, lead_left, lead_right, eta_device, device_to_lead_left,
+                                 device_to_lead_right, omega_scale, max_channel_factor)
+        tasks.append((i, w, w_cm1, name, tuple(float(e) for e in ladder)))
+
+    # ladder state
+    state = {}
+    for i, w, w_cm1, name, ladder in tasks:
+        K = len(meshes[name].kpoints)
+        state[i] = {"pending": list(range(K)), "accepted": {}, "attempts": [], "done": False, "rej_all": [],
+                    "K": K, "name": name, "w": w, "ladder": ladder}
+    rung = 0
+    while True:
+        batch: dict[str, list] = {}
+        for i, w, w_cm1, name, ladder in tasks:
+            s = state[i]
+            if s["done"] or rung >= len(ladder) or not s["pending"]:
+                continue
+            for ki in s["pending"]:
+                batch.setdefault(name, []).append((i, ki, ladder[rung]))
+        if not batch:
+            break
+        for name, pts in batch.items():
+            mesh = meshes[name]
+            T, st = _solve(mesh, [state[i]["w"] for i, _, _ in pts], [e for _, _, e in pts], [k for _, k, _ in pts])
+            outcome: dict[int, list] = {}
+            for (i, ki, eta), t, sv in zip(pts, T, st):
+                outcome.setdefault(i, []).append((ki, eta, t, sv))
+            for i, rows in outcome.items():
+                s = state[i]
+                kpts = mesh.kpoints
+                if per_k:
+                    nxt = []
+                    for ki, eta, t, sv in rows:
+                        reason = _classify(t, sv, mesh.max_allowed, nonnegative_tolerance)
+                        if reason is None:
+                            s["accepted"][ki] = (float(max(t, 0.0)), float(eta))
+                        else:
+                            s["attempts"].append((ki, rung, _rejected(s["w"], kpts[ki], eta, t, reason)))
+                            nxt.append(ki)
+                    s["pending"] = nxt
+                else:
+                    good = []
+                    for ki, eta, t, sv in rows:
+                        reason = _classify(t, sv, mesh.max_allowed, nonnegative_tolerance)
+                        if reason is None:
+                            good.append(float(max(t, 0.0)))
+                        elif collect_rejected:
+                            s["rej_all"].append(_rejected(s["w"], kpts[ki], eta, t, reason))
+                    frac = float(len(good) / s["K"])
+                    if good and frac >= min_success_fraction:
+                        eta = rows[0][1]
+                        s["done"] = True
+                        s["value"] = float(np.mean(good))
+                        s["info"] = {"n_total": s["K"], "n_success": len(good), "n_failed": s["K"] - len(good),
+                                     "success_fraction": frac, "eta_selected": float(eta),
+                                     "eta_histogram": {float(e): (len(good) if float(e) == float(eta) else 0)
+                                                       for e in s["ladder"]}}
+                        if collect_rejected:
+                            s["info"]["n_rejected"] = len(s["rej_all"])
+                            s["info"]["rejected"] = s["rej_all"]
+        rung += 1
+
+    for i, w, w_cm1, name, ladder in tasks:
+        s = state[i]
+        try:
+            if per_k:
+                K = s["K"]
+                acc = s["accepted"]
+                v = [acc[k][0] for k in range(K) if k in acc]
+                used = [acc[k][1] for k in range(K) if k in acc]
+                frac = float(len(v) / K)
+                if not v:
+                    raise RuntimeError("No k-point converged for adaptive k-averaged transmission.")
+                if frac < min_success_fraction:
+                    raise RuntimeError("Adaptive k-averaged transmission failed success-fraction threshold "
+                                       f"(got {frac:.3f}, required >= {min_success_fraction:.3f}).")
+                info = {"n_total": K, "n_success": len(v), "n_failed": K - len(v), "success_fraction": frac,
+                        "eta_histogram": {float(e): int(sum(1 for u in used if u == float(e))) for e in ladder}}
+                if collect_rejected:
+                    rej = [a[2] for a in sorted(s["attempts"], key=lambda a: (a[0], a[1]))]
+                    info["n_rejected"] = len(rej)
+                    info["rejected"] = rej
+                tval = float(np.mean(v))
+            else:
+                if not s["done"]:
+                    raise RuntimeError("No eta value satisfied global adaptive k-averaging quality threshold "
+                                       f"(required success_fraction >= {min_success_fraction:.3f}).")
+                info, tval = s["info"], s["value"]
+        except Exception as exc:
+            results[i] = {"value": np.nan, "eta_record": None,
+                          "failure": {"omega_qe": w, "omega_cm1": w_cm1, "error": str(exc)}}
+            continue
+        hist = dict(info.get("eta_histogram", {}))
+        used_e = [float(e) for e, c in hist.items() if int(c) > 0]
+        max_eta_used = max(used_e) if used_e else np.nan
+        results[i] = {
+            "value": tval,
+            "eta_record": {
+                "omega_qe": w, "omega_cm1": w_cm1, "n_failed_kpoints": int(info.get("n_failed", 0)),
+                "success_fraction": float(info.get("success_fraction", 0.0)), "eta_histogram": hist,
+                "eta_selected": info.get("eta_selected", None),
+                "max_eta_used": None if not np.isfinite(max_eta_used) else float(max_eta_used),
+                "max_eta_over_omega": None if not np.isfinite(max_eta_used) else float(max_eta_used / w),
+            },
+            "failure": None,
+            "n_rejected": int(info.get("n_rejected", 0)) if collect_rejected else 0,
+        }
+
+    rejected_total = 0
+    for i, r in enumerate(results):
+        vals[i] = float(r["value"])
+        if r["failure"] is None and collect_rejected:
+            rejected_total += int(r.get("n_rejected", 0))
+    eta_records = [r["eta_record"] for r in results if r["eta_record"] is not None]
+    omega_failures = [r["failure"] for r in results if r["failure"] is not None]
+    if np.all(~np.isfinite(vals)):
+        raise RuntimeError("Transmission calculation failed for all omega points.")
+    vals = np.where(np.isfinite(vals), vals, np.nan)
+    vals = np.where(vals < 0.0, np.maximum(vals, -1e-12), vals)
+    vals = np.where(np.isfinite(vals), np.clip(vals, 0.0, None), np.nan)
+    max_ratio = max((r["max_eta_over_omega"] for r in eta_records if r["max_eta_over_omega"] is not None),
+                    default=None)
+    return {
+        "values": vals,
+        "eta_records": eta_records,
+        "omega_failures": omega_failures,
+        "n_rejected_total": int(rejected_total),
+        "summary": {
+            "surface_gf_method": sgf_method,
+            "eta_scheme": eta_scheme,
+            "eta_fixed": eta_fixed,
+            "eta_values_base": eta_values_base,
+            "eta_device": eta_device,
+            "parallel": {"enabled": bool(parallel_cfg["enabled"]), "backend": str(parallel_cfg["backend"]),
+                         "workers": int(parallel_cfg["workers"]), "blas_threads": parallel_cfg["blas_threads"]},
+            "max_eta_over_omega": max_ratio,
+            "n_omega_failures": len(omega_failures),
+        },
+    }

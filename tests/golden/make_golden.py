@@ -107,10 +107,58 @@ def green(out_dir: Path) -> None:
     np.savez_compressed(out_dir / "green.npz", **out)
 
 
+WORKFLOW_OMEGAS = [-0.1, 0.0, 0.3, 0.7, 1.1, 1.8, 2.5, 3.3]
+WORKFLOW_KMESH = {"low_cm1": 1e5, "low": {"kpoints": [(0.0,), (1.2,)]}, "high": {"kpoints": [(-2.0,), (0.4,), (2.6,)]}}
+WORKFLOW_CFGS = {
+    "adaptive": {"solver": {"surface_gf_method": "sancho_rubio", "eta_scheme": "adaptive",
+                            "eta_values": [1e-7, 1e-5, 1e-3], "max_channel_factor": 0.15,
+                            "min_success_fraction": 0.3, "collect_rejected": True}},
+    "global": {"solver": {"surface_gf_method": "sancho_rubio", "eta_scheme": "adaptive-global",
+                          "eta_values": [1e-7, 1e-5, 1e-3], "max_channel_factor": 0.2,
+                          "min_success_fraction": 0.6, "collect_rejected": True, "max_eta_over_omega": 1e-4,
+                          "eta_ratio_cm1_min": 5e4, "eta_device": 2e-6}},
+    "fixed": {"solver": {"surface_gf_method": "sancho_rubio", "eta_scheme": "fixed", "eta_fixed": 3e-6,
+                         "omega_scale_mode": "ev", "parallel": {"enabled": True, "workers": 4}}},
+    "strict": {"solver": {"surface_gf_method": "sancho_rubio", "eta_scheme": "adaptive", "eta_values": [1e-7, 1e-5],
+                          "max_channel_factor": 0.08, "min_success_fraction": 1.0}},
+    "strict_global": {"solver": {"surface_gf_method": "sancho_rubio", "eta_scheme": "adaptive_global",
+                                 "eta_values": [1e-7, 1e-5], "max_channel_factor": 0.08,
+                                 "min_success_fraction": 1.0, "collect_rejected": True}},
+}
+
+
+def workflow_system(params_cls, lead_fn, dev_fn):
+    """The small slab of the workflow fixture (seeded spring network, 4 layers)."""
+    from negfpy_b200 import workloads as W
+
+    p = W.spring_network(2, ny=2, nz=8, periodic_y=True, periodic_z=False)
+    prm = params_cls(masses=p.masses, fc00_terms=p.fc00_terms, fc01_terms=p.fc01_terms, dof_per_atom=3)
+    return dev_fn(4, prm), lead_fn(prm)
+
+
+def workflow(out_dir: Path) -> None:
+    """workflow.npz: negfpy's _run_transmission (workflows/ifc_bulk.py:1059-1288) on a small slab."""
+    import json
+
+    from negfpy.models.material_kspace import MaterialKspaceParams, material_kspace_device, material_kspace_lead
+    from negfpy.workflows import ifc_bulk
+
+    dev, lead = workflow_system(MaterialKspaceParams, material_kspace_lead, material_kspace_device)
+    out = {}
+    for name, cfg in WORKFLOW_CFGS.items():
+        res = ifc_bulk._run_transmission(cfg, device=dev, lead_left=lead, lead_right=lead,
+                                         omegas=np.array(WORKFLOW_OMEGAS), kmesh=WORKFLOW_KMESH)
+        out[name + "_values"] = res["values"]
+        meta = {k: res[k] for k in ("eta_records", "omega_failures", "n_rejected_total", "summary")}
+        out[name + "_meta"] = np.array(json.dumps(meta, default=lambda o: list(o) if isinstance(o, tuple) else o))
+    np.savez_compressed(out_dir / "workflow.npz", **out)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference/src")
-    ap.add_argument("--only", choices=["thermal", "green"], default=None, help="write one fixture file only")
+    ap.add_argument("--only", choices=["thermal", "green", "workflow"], default=None,
+                    help="write one fixture file only")
     args = ap.parse_args()
     sys.path.insert(0, args.ref)
     if args.only == "thermal":
@@ -120,6 +168,10 @@ def main() -> None:
     if args.only == "green":
         green(OUT)
         print("wrote green.npz")
+        return
+    if args.only == "workflow":
+        workflow(OUT)
+        print("wrote workflow.npz")
         return
     import negfpy.core as R
     from negfpy.core.types import Device1D, LeadBlocks
@@ -235,6 +287,7 @@ def main() -> None:
     np.savez_compressed(OUT / "cases.npz", **cases)
     thermal(OUT)
     green(OUT)
+    workflow(OUT)
     print("wrote", sorted(p.name for p in OUT.glob("*.npz")))
 
 
