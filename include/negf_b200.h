@@ -283,6 +283,19 @@ int negf_kappa_f64(const double* omega, const double* t_mean, int n_omega, const
                    double omega_unit_rad_s, double* kappa_out, void* stream);
 
 /*
+ * k-space blocks of a force-constant model for n_k k-points at once:
+ *   out[k] = diag(row_weight) (sum_t terms[t] exp(i (ky dy_t + kz dz_t)) + pinning I) diag(col_weight)
+ * with real terms[n_terms][n][n], shifts[n_terms][2] = (dy, dz) and
+ * kpoints[n_k][2] = (ky, kz); out is complex128 [n_k][n][n].  Replaces the
+ * per-k phase sums and mass weighting of negfpy
+ * models/material_kspace.py:99-128 (_sum_k_terms, _build_dynamical_blocks).
+ * At most 256 terms.  Returns NEGF_EINVAL on a bad argument.
+ */
+int negf_kspace_blocks_f64(const double* terms, const double* shifts, int n_terms, const double* kpoints, int n_k,
+                           int n, const double* row_weight, const double* col_weight, double pinning, double* out,
+                           void* stream);
+
+/*
  * k moments of an omega-major [n_omega][n_k] transmission table:
  * t_mean[w] = <T>_k, t2_mean[w] = <T^2>_k.  Replaces the per-omega moments
  * of negfpy workflows/ifc_bulk.py:1690-1784 (full counting statistics).

@@ -71,6 +71,7 @@ _SIGNATURES = {
     "negf_kavg_f64": (_I, [_P, _I, _I, _P, _P]),
     "negf_heat_current_f64": (_I, [_P, _P, _I, _I, _D, _D, _P, _P]),
     "negf_kmoments_f64": (_I, [_P, _I, _I, _P, _P, _P]),
+    "negf_kspace_blocks_f64": (_I, [_P, _P, _I, _P, _I, _I, _P, _P, _D, _P, _P]),
     "negf_fcs_cumulants_f64": (_I, [_P, _P, _P, _I, _D, _D, _P, _P]),
     "negf_kappa_f64": (_I, [_P, _P, _I, _P, _I, _D, _P, _P]),
 }

@@ -195,6 +195,7 @@ def material_kspace_lead(params: MaterialKspaceParams) -> LeadKSpace:
     def _builder(kpar: KPar):
         return _blocks_at(params, kpar, params.masses, params.masses)
 
+    _builder.kspace_params = params  # lets the batched path build every k on the GPU
     return LeadKSpace(blocks_builder=_builder)
 
 
@@ -215,4 +216,6 @@ def material_kspace_device(n_layers: int, params: MaterialKspaceParams, layer_ma
         st = material_kspace_stack(params, [kpar if kpar is not None else ()], layer_masses=masses, n_layers=n_layers)
         return Device1D(onsite_blocks=list(st["onsite"][0]), coupling_blocks=list(st["coupling"][0]))
 
+    _builder.kspace_params = params
+    _builder.kspace_device = {"n_layers": int(n_layers), "layer_masses": None if layer_masses is None else masses}
     return DeviceKSpace(device_builder=_builder)

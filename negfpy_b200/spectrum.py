@@ -19,13 +19,36 @@ from .surface_gf import check_method
 def system_over_k(device, lead_left, lead_right, kpoints, eta_device=None, device_to_lead_left=None,
                   device_to_lead_right=None, contact_left_indices=None, contact_right_indices=None,
                   omega_scale=None) -> engine.StackedSystem:
-    """Resolve and upload the blocks of every k once (omega-independent)."""
+    """Resolve and upload the blocks of every k once (omega-independent).
+
+    Material lead / device / same lead with default couplings and contacts
+    and no omega_scale: every k is built on the GPU (``kspace.stacked_system``)."""
     ks = [None] if kpoints is None else list(kpoints)
+    fast = _material_fast_path(device, lead_left, lead_right, device_to_lead_left, device_to_lead_right,
+                               contact_left_indices, contact_right_indices, omega_scale)
+    if fast is not None:
+        from .kspace import stacked_system
+
+        return stacked_system(fast[0], fast[1], [() if k is None else k for k in ks])
     systems = [point_system(1.0, device, lead_left, lead_right, 1.0, eta_device, k, device_to_lead_left,
                             device_to_lead_right, contact_left_indices, contact_right_indices, omega_scale)
                for k in ks]
     sysobj, _ = stack_systems(systems)
     return sysobj
+
+
+def _material_fast_path(device, lead_left, lead_right, vdl_left, vdl_right, idx_l, idx_r, omega_scale):
+    """(params, device info) when the GPU block builder reproduces the host path exactly in scope."""
+    if any(x is not None for x in (vdl_left, vdl_right, idx_l, idx_r, omega_scale)):
+        return None
+    lb = getattr(getattr(lead_left, "blocks_builder", None), "kspace_params", None)
+    rb = getattr(getattr(lead_right, "blocks_builder", None), "kspace_params", None)
+    db = getattr(device, "device_builder", None)
+    dp = getattr(db, "kspace_params", None)
+    info = getattr(db, "kspace_device", None)
+    if lb is None or lb is not rb or dp is not lb or info is None:
+        return None
+    return lb, info
 
 
 def grid_points(W: int, K: int, device=None):
