@@ -553,7 +553,18 @@ def main():
     nl = n
     h2d = (3 * K * nl * nl + K * n * n * 2 + 2 * K * n * nl) * 16 + P * (8 + 8 + 8 + 4)
     d2h = P * (8 + 4 + 4 + 4)
-    e2e_diff = float(np.max(np.abs(res["T"].ravel() - T.cpu().numpy()) / np.maximum(np.abs(T.cpu().numpy()), 1)))
+    t_dev = T.cpu().numpy()
+    e2e_rel = np.abs(res["T"].ravel() - t_dev) / np.maximum(np.abs(t_dev), 1)
+    e2e_diff = float(e2e_rel.max())
+    # The two runs see blocks that differ by rounding (host vs GPU phase sums);
+    # at band-edge points the decimation amplifies that to ~1e-6 in T, in
+    # negfpy's algorithm as much as here, while kappa integrates it away.
+    k_e2e, k_dev = (float(nb.kappa_from_grid(wl.omegas[shard], t.reshape(W, K), [300.0], wl.omega_unit_rad_s)[0])
+                    for t in (res["T"], t_dev))
+    e2e_cmp = {"max_rel_diff_vs_device_run": e2e_diff,
+               "points_rel_diff_above_1e-10": int((e2e_rel > 1e-10).sum()),
+               "points_rel_diff_above_1e-8": int((e2e_rel > 1e-8).sum()),
+               "kappa_300K_rel_diff_vs_device_run": abs(k_e2e - k_dev) / abs(k_dev)}
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -580,7 +591,7 @@ def main():
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_val, "unit": "points/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h), "api": "negfpy_b200.transmission_grid (LeadKSpace/DeviceKSpace)",
-                    "max_rel_diff_vs_device_run": e2e_diff},
+                    **e2e_cmp},
             "gpu_launches": 2 * args.steps,
             "status_ok_fraction": float(np.mean(status == 0)),
             "clocks": clk.summary(),
