@@ -193,6 +193,10 @@ static __device__ int gj_invert32(float2* X, float2* Y, int n, int NP, const GJS
     if (lane == 0 && key0) atomicMax(&sh.key[0], key0);
     __syncthreads();
     float2 lam = make_float2(1.f, 0.f);
+    // Bit i: row (tid >> 3) + 32 i (this thread's rows; its column is
+    // tid & 7) was a pivot row of this panel.
+    static_assert(kThreads == 256, "rows of a thread are 32 apart");
+    unsigned used_rows = 0u;
     for (int j = 0; j < jmax; ++j) {
       const unsigned key = sh.key[j];
       if ((key >> 23) >= 0xffu) return kNonFinite;
@@ -212,8 +216,9 @@ static __device__ int gj_invert32(float2* X, float2* Y, int n, int NP, const GJS
       }
       const float2 piv = P[pr * 8 + j];
       const float2 ps = make_float2(piv.x * sc, piv.y * sc);
+      if ((pr & 31) == (tid >> 3)) used_rows |= 1u << (pr >> 5);
       unsigned nk = 0u;
-      for (int e = tid; e < PE; e += kThreads) {
+      for (int e = tid, i = 0; e < PE; e += kThreads, ++i) {
         const int r = e >> 3, c = e & 7;
         const bool isp = (r == pr);
         const float2 fv = P[r * 8 + j], mv = P[pr * 8 + c], av = P[e];
@@ -223,11 +228,7 @@ static __device__ int gj_invert32(float2* X, float2* Y, int n, int NP, const GJS
         float2 v = fneg(fmulc(b, m));
         if (!isp && c != j) cfma(v, ps, av);
         Pn[e] = v;
-        if (c == j + 1 && r >= k0 && r < n) {
-          bool used = isp;
-          for (int i = 0; i < j; ++i) used = used || (sh.sig[k0 + i] == r);
-          if (!used) nk = max(nk, pivot_key32(v, r));
-        }
+        if (c == j + 1 && r >= k0 && r < n && !((used_rows >> i) & 1u)) nk = max(nk, pivot_key32(v, r));
       }
       lam = fmulc(lam, ps);
       if (j + 1 < jmax) {

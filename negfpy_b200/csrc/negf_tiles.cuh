@@ -174,6 +174,10 @@ static __device__ int gj_invert_global(double2* X, double2* Y, int n, int NP, co
     if (lane == 0 && key0) atomicMax(&sh.key[0], key0);
     __syncthreads();
     double2 lam = make_double2(1.0, 0.0);
+    // Bit i: row (tid >> 3) + 32 i (this thread's rows; its column is
+    // tid & 7) was a pivot row of this panel.
+    static_assert(kThreads == 256, "rows of a thread are 32 apart");
+    unsigned used_rows = 0u;
     for (int j = 0; j < jmax; ++j) {
       const unsigned key = sh.key[j];
       if ((key >> 20) >= 0x7ffu) return kNonFinite;
@@ -193,11 +197,11 @@ static __device__ int gj_invert_global(double2* X, double2* Y, int n, int NP, co
       }
       const double2 piv = P[pr * 8 + j];
       const double2 ps = make_double2(piv.x * sc, piv.y * sc);
+      if ((pr & 31) == (tid >> 3)) used_rows |= 1u << (pr >> 5);
       unsigned nk = 0u;
-      for (int e = tid; e < PE; e += kThreads) {
+      for (int e = tid, i = 0; e < PE; e += kThreads, ++i) {
         const int r = e >> 3, c = e & 7;
         const bool isp = (r == pr);
-        // rows already used as pivots in this panel are sig[k0..k0+j]
         const double2 fv = P[r * 8 + j], mv = P[pr * 8 + c], av = P[e];
         const double2 bb = isp ? cneg(lam) : fv;
         const double2 b = make_double2(bb.x * sc, bb.y * sc);
@@ -205,11 +209,7 @@ static __device__ int gj_invert_global(double2* X, double2* Y, int n, int NP, co
         double2 v = cneg(cmul(b, m));
         if (!isp && c != j) cfma(v, ps, av);
         Pn[e] = v;
-        if (c == j + 1 && r >= k0 && r < n) {
-          bool used = isp;
-          for (int i = 0; i < j; ++i) used = used || (sh.sig[k0 + i] == r);
-          if (!used) nk = max(nk, pivot_key8(v, r));
-        }
+        if (c == j + 1 && r >= k0 && r < n && !((used_rows >> i) & 1u)) nk = max(nk, pivot_key8(v, r));
       }
       lam = cmul(lam, ps);
       if (j + 1 < jmax) {
