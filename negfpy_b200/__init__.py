@@ -43,6 +43,7 @@ from .models import (
     device_mass_defect,
     device_perfect_chain,
     lead_blocks,
+    interface_contacts,
     material_kspace_device,
     material_kspace_lead,
 )

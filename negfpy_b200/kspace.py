@@ -13,14 +13,22 @@ import numpy as np
 import torch
 
 from . import _lib, engine
-from .models import MaterialKspaceParams, parse_ky_kz
+from .models import MaterialKspaceParams, interface_terms, parse_ky_kz
+
+
+def real_terms(*groups) -> bool:
+    """True when every force-constant block is real (the kernel's operand type)."""
+    return all(not np.iscomplexobj(v) or not np.any(np.imag(v)) for g in groups if g is not None for v in g.values())
 
 
 def _phase_sum(terms: dict, kpts: torch.Tensor, wr: torch.Tensor, wc: torch.Tensor, pin: float) -> torch.Tensor:
+    if not real_terms(terms):
+        raise ValueError("negf_kspace_blocks_f64 takes real force-constant blocks; complex ones need the host builder")
     lib = _lib.load()
     dev = kpts.device
     keys = list(terms.keys())
-    blocks = torch.as_tensor(np.stack([np.asarray(terms[k], dtype=float) for k in keys]), device=dev).contiguous()
+    blocks = torch.as_tensor(np.stack([np.real(np.asarray(terms[k])).astype(float) for k in keys]),
+                             device=dev).contiguous()
     shifts = torch.as_tensor(np.asarray(keys, dtype=float), device=dev).contiguous()
     K, n = kpts.shape[0], blocks.shape[-1]
     out = torch.empty((K, n, n), dtype=torch.complex128, device=dev)
@@ -70,3 +78,24 @@ def stacked_system(lead_params: MaterialKspaceParams, device_info: dict, kpoints
     lead = (st["d00"], st["d01"], st["d10"])
     return engine.StackedSystem(lead, lead, st["onsite"].contiguous(), st["coupling"].contiguous(),
                                 int(device_info["n_layers"]), st["d10"], st["d01"], True)
+
+
+def interface_system(params: MaterialKspaceParams, device_info: dict, kpoints) -> engine.StackedSystem:
+    """StackedSystem of the IFC transport set-up of ``models.interface_contacts``
+    (negfpy ``workflows/ifc_bulk.py:690-742``) around a material device: all
+    k blocks of both leads, the device and the couplings V_R = d01 of the
+    right lead, V_L = V_R^H, built on the GPU."""
+    st = kspace_stack(params, kpoints, device_info["n_layers"], device_info["layer_masses"])
+    dev = st["d00"].device
+    kk = [parse_ky_kz(k) for k in kpoints]
+    kpts = torch.as_tensor(np.asarray(kk, dtype=float).reshape(-1, 2), device=dev).contiguous()
+    w = torch.as_tensor(1.0 / np.sqrt(np.repeat(np.asarray(params.masses, dtype=float), params.dof_per_atom)),
+                        device=dev)
+    left_terms, right_terms = interface_terms(params)
+    d01l = _phase_sum(left_terms, kpts, w, w, 0.0)
+    d01r = _phase_sum(right_terms, kpts, w, w, 0.0)
+    herm = lambda a: a.conj().transpose(-1, -2).contiguous()  # noqa: E731
+    lead_l = (st["d00"], d01l, herm(d01l))
+    lead_r = (st["d00"], d01r, herm(d01r))
+    return engine.StackedSystem(lead_l, lead_r, st["onsite"].contiguous(), st["coupling"].contiguous(),
+                                int(device_info["n_layers"]), herm(d01r), d01r, False)

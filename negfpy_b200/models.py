@@ -219,3 +219,61 @@ def material_kspace_device(n_layers: int, params: MaterialKspaceParams, layer_ma
     _builder.kspace_params = params
     _builder.kspace_device = {"n_layers": int(n_layers), "layer_masses": None if layer_masses is None else masses}
     return DeviceKSpace(device_builder=_builder)
+
+
+def interface_terms(params: MaterialKspaceParams) -> tuple[dict, dict]:
+    """Force-constant terms of the two lead couplings of the IFC transport
+    set-up (negfpy ``workflows/ifc_bulk.py:690-711``): ``(left, right)``.
+
+    With FC10 the given fc10 terms, or {(-dy, -dz): FC01(dy, dz)^H} when
+    there are none, the left lead's d01 sums FC10(dy, dz) and the right
+    lead's sums FC10(dy, dz)^T at the shift (-dy, -dz).
+    """
+    if params.fc10_terms is None:
+        fc10 = {(-dy, -dz): np.asarray(v, dtype=np.complex128).conj().T for (dy, dz), v in params.fc01_terms.items()}
+    else:
+        fc10 = {key: np.asarray(v, dtype=np.complex128) for key, v in params.fc10_terms.items()}
+    right = {(-dy, -dz): v.T for (dy, dz), v in fc10.items()}
+    return dict(fc10), right
+
+
+def interface_contacts(params: MaterialKspaceParams):
+    """Leads and device couplings of the IFC transport set-up, as negfpy's
+    ``_build_interface_contacts`` (``workflows/ifc_bulk.py:690-742``).
+
+    Returns ``(lead_left, lead_right, device_to_lead_left, device_to_lead_right)``:
+    two ``LeadKSpace`` with blocks (d00, d01, d01^H), where d00 = M (Phi00(k)
+    + pinning) M and d01 = M K01(k) M over the terms of ``interface_terms``
+    (M = diag(m^-1/2)), and the couplings V_R(k) = d01 of the right lead and
+    V_L(k) = V_R(k)^H.  Each builder is tagged so that the batched path can
+    build every k of the same set-up on the GPU.
+    """
+    left_terms, right_terms = interface_terms(params)
+    m = _inv_sqrt_mass(params.masses, params.dof_per_atom)
+    pin = float(params.onsite_pinning)
+
+    def _weighted(terms: dict, kpar: KPar, pinning: float = 0.0) -> Array:
+        ky, kz = parse_ky_kz(kpar)
+        phi = _phase_sum_stack(terms, np.array([ky]), np.array([kz]))[0]
+        if pinning != 0.0:
+            phi = phi + pinning * np.eye(params.ndof, dtype=np.complex128)
+        return m[:, None] * phi * m[None, :]
+
+    def _lead(terms: dict):
+        def _builder(kpar: KPar):
+            d00 = _weighted(params.fc00_terms, kpar, pin)
+            d01 = _weighted(terms, kpar)
+            return d00, d01, d01.conj().T
+        return _builder
+
+    def _vdl_right(kpar: KPar) -> Array:
+        return _weighted(right_terms, kpar)
+
+    def _vdl_left(kpar: KPar) -> Array:
+        return _vdl_right(kpar).conj().T
+
+    token = object()  # ties the four pieces of one set-up together
+    left, right = _lead(left_terms), _lead(right_terms)
+    for fn, role in ((left, "left"), (right, "right"), (_vdl_left, "vdl_left"), (_vdl_right, "vdl_right")):
+        fn.kspace_interface = (token, params, role)
+    return LeadKSpace(blocks_builder=left), LeadKSpace(blocks_builder=right), _vdl_left, _vdl_right

@@ -27,9 +27,10 @@ def system_over_k(device, lead_left, lead_right, kpoints, eta_device=None, devic
     fast = _material_fast_path(device, lead_left, lead_right, device_to_lead_left, device_to_lead_right,
                                contact_left_indices, contact_right_indices, omega_scale)
     if fast is not None:
-        from .kspace import stacked_system
+        from .kspace import interface_system, stacked_system
 
-        return stacked_system(fast[0], fast[1], [() if k is None else k for k in ks])
+        build = interface_system if fast[0] == "interface" else stacked_system
+        return build(fast[1], fast[2], [() if k is None else k for k in ks])
     systems = [point_system(1.0, device, lead_left, lead_right, 1.0, eta_device, k, device_to_lead_left,
                             device_to_lead_right, contact_left_indices, contact_right_indices, omega_scale)
                for k in ks]
@@ -38,17 +39,34 @@ def system_over_k(device, lead_left, lead_right, kpoints, eta_device=None, devic
 
 
 def _material_fast_path(device, lead_left, lead_right, vdl_left, vdl_right, idx_l, idx_r, omega_scale):
-    """(params, device info) when the GPU block builder reproduces the host path exactly in scope."""
-    if any(x is not None for x in (vdl_left, vdl_right, idx_l, idx_r, omega_scale)):
+    """(kind, params, device info) when the GPU block builder covers the system:
+    kind "material" for ``material_kspace_lead`` leads with the default
+    couplings, "interface" for the four pieces of one ``interface_contacts``
+    set-up; both around ``material_kspace_device`` of the same parameters,
+    with default contacts, no omega scale and real force constants."""
+    from .kspace import real_terms
+
+    if any(x is not None for x in (idx_l, idx_r, omega_scale)):
         return None
-    lb = getattr(getattr(lead_left, "blocks_builder", None), "kspace_params", None)
-    rb = getattr(getattr(lead_right, "blocks_builder", None), "kspace_params", None)
     db = getattr(device, "device_builder", None)
     dp = getattr(db, "kspace_params", None)
     info = getattr(db, "kspace_device", None)
-    if lb is None or lb is not rb or dp is not lb or info is None:
+    if dp is None or info is None or not real_terms(dp.fc00_terms, dp.fc01_terms, dp.fc10_terms):
         return None
-    return lb, info
+    if vdl_left is None and vdl_right is None:
+        lb = getattr(getattr(lead_left, "blocks_builder", None), "kspace_params", None)
+        rb = getattr(getattr(lead_right, "blocks_builder", None), "kspace_params", None)
+        return ("material", dp, info) if lb is dp and rb is dp else None
+    tags = [getattr(x, "kspace_interface", None) for x in (getattr(lead_left, "blocks_builder", None),
+                                                          getattr(lead_right, "blocks_builder", None),
+                                                          vdl_left, vdl_right)]
+    if any(t is None for t in tags):
+        return None
+    token = tags[0][0]
+    roles = ["left", "right", "vdl_left", "vdl_right"]
+    if all(t[0] is token and t[1] is dp and t[2] == r for t, r in zip(tags, roles)):
+        return "interface", dp, info
+    return None
 
 
 def grid_points(W: int, K: int, device=None):

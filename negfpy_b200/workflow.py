@@ -25,8 +25,13 @@ import numpy as np
 import torch
 
 from . import _lib
+from .models import interface_contacts
 from .negf import _check_adaptive_args, _classify, _prepare_ladder_systems, stack_systems
+from .spectrum import _material_fast_path
 from .surface_gf import check_method
+
+# negfpy's name for the IFC transport set-up (workflows/ifc_bulk.py:690-742).
+_build_interface_contacts = interface_contacts
 
 # CODATA 2018 constants, as negfpy modeling/units.py:8-16.
 RYDBERG_J = 2.1798723611035e-18
@@ -89,9 +94,20 @@ class _Mesh:
     def __init__(self, kpoints, device, lead_left, lead_right, eta_device, vdl_left, vdl_right, omega_scale,
                  max_channel_factor):
         self.kpoints = list(kpoints)
-        systems = _prepare_ladder_systems(1.0, device, lead_left, lead_right, self.kpoints, eta_device, vdl_left,
-                                          vdl_right, None, None, omega_scale)
-        self.sys, _ = stack_systems(systems)
+        fast = _material_fast_path(device, lead_left, lead_right, vdl_left, vdl_right, None, None, omega_scale)
+        if fast is not None and self.kpoints:
+            # All k blocks on the GPU; one k through the host path for the
+            # validation, the omega scale and the device-eta rule.
+            from .kspace import interface_system, stacked_system
+
+            systems = _prepare_ladder_systems(1.0, device, lead_left, lead_right, self.kpoints[:1], eta_device,
+                                              vdl_left, vdl_right, None, None, omega_scale)
+            build = interface_system if fast[0] == "interface" else stacked_system
+            self.sys = build(fast[1], fast[2], [() if k is None else k for k in self.kpoints])
+        else:
+            systems = _prepare_ladder_systems(1.0, device, lead_left, lead_right, self.kpoints, eta_device, vdl_left,
+                                              vdl_right, None, None, omega_scale)
+            self.sys, _ = stack_systems(systems)
         self.scale = systems[0]["scale"]
         self.eta_dev_for = systems[0]["_eta_dev_for"]
         nl = int(self.sys.nl)

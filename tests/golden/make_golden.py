@@ -154,10 +154,85 @@ def workflow(out_dir: Path) -> None:
     np.savez_compressed(out_dir / "workflow.npz", **out)
 
 
+INTERFACE_KPOINTS = {"slab": [(-2.7,), (-0.4,), (0.0,), (1.3,), (3.0,)],
+                     "bulk": [(0.0, 0.0), (0.7, -1.9), (-2.2, 2.9)]}
+INTERFACE_LAYERS = {"slab": 4, "bulk": 3}
+INTERFACE_FRACTIONS = (0.13, 0.41, 0.77)  # omega / omega_max of the T points
+
+
+def interface_params(name: str, params_cls):
+    """Seeded force-constant sets of the interface fixture: ``slab`` (n = 48,
+    1D k, fc10 implied by fc01) and ``bulk`` (n = 12, 2D k, explicit fc10
+    terms and an onsite pinning)."""
+    from negfpy_b200 import workloads as W
+
+    if name == "slab":
+        p = W.spring_network(2, ny=2, nz=8, periodic_y=True, periodic_z=False)
+        return params_cls(masses=p.masses, fc00_terms=p.fc00_terms, fc01_terms=p.fc01_terms, dof_per_atom=3)
+    p = W.spring_network(3, ny=2, nz=2, periodic_y=True, periodic_z=True)
+    fc10 = {(-dy, -dz): np.asarray(v).T.copy() for (dy, dz), v in p.fc01_terms.items()}
+    return params_cls(masses=p.masses, fc00_terms=p.fc00_terms, fc01_terms=p.fc01_terms, fc10_terms=fc10,
+                      dof_per_atom=3, onsite_pinning=0.02)
+
+
+def _terms_arrays(prefix: str, terms) -> dict:
+    if terms is None:
+        return {}
+    keys = list(terms.keys())
+    return {prefix + "_keys": np.array(keys, dtype=np.int64), prefix + "_blocks": np.stack([terms[k] for k in keys])}
+
+
+def interface(out_dir: Path) -> None:
+    """interface.npz: negfpy's _build_interface_contacts (workflows/ifc_bulk.py:690-742),
+    transmission through it, and _run_transmission on the slab set-up."""
+    import json
+
+    import negfpy.core as R
+    from negfpy.models.material_kspace import MaterialKspaceParams, material_kspace_device
+    from negfpy.workflows import ifc_bulk
+
+    from negfpy_b200 import workloads as W
+
+    out = {}
+    for name in ("slab", "bulk"):
+        prm = interface_params(name, MaterialKspaceParams)
+        ll, lr, vdl_l, vdl_r = ifc_bulk._build_interface_contacts(prm)
+        kp = INTERFACE_KPOINTS[name]
+        blocks = {"l": [ll.blocks(k) for k in kp], "r": [lr.blocks(k) for k in kp]}
+        for side in ("l", "r"):
+            for i, key in enumerate(("d00", "d01", "d10")):
+                out[f"{name}_{side}_{key}"] = np.stack([b[i] for b in blocks[side]])
+        out[f"{name}_vl"] = np.stack([vdl_l(k) for k in kp])
+        out[f"{name}_vr"] = np.stack([vdl_r(k) for k in kp])
+        out[f"{name}_masses"] = np.asarray(prm.masses, dtype=float)
+        out[f"{name}_pinning"] = float(prm.onsite_pinning)
+        out.update(_terms_arrays(f"{name}_fc00", prm.fc00_terms))
+        out.update(_terms_arrays(f"{name}_fc01", prm.fc01_terms))
+        out.update(_terms_arrays(f"{name}_fc10", prm.fc10_terms))
+        wmax = W.estimate_omega_max(prm, nk=6, two_d=(name == "bulk"))
+        eta = 1e-5 * wmax * wmax
+        dev = material_kspace_device(n_layers=INTERFACE_LAYERS[name], params=prm)
+        om = np.array([f * wmax for f in INTERFACE_FRACTIONS])
+        out[f"{name}_omegas"] = om
+        out[f"{name}_eta"] = eta
+        out[f"{name}_T"] = np.array([[R.transmission(float(w), dev, ll, lr, eta=eta, kpar=k, device_to_lead_left=vdl_l,
+                                                     device_to_lead_right=vdl_r) for k in kp] for w in om])
+    prm = interface_params("slab", MaterialKspaceParams)
+    ll, lr, vdl_l, vdl_r = ifc_bulk._build_interface_contacts(prm)
+    dev = material_kspace_device(n_layers=4, params=prm)
+    res = ifc_bulk._run_transmission(WORKFLOW_CFGS["adaptive"], device=dev, lead_left=ll, lead_right=lr,
+                                     device_to_lead_left=vdl_l, device_to_lead_right=vdl_r,
+                                     omegas=np.array(WORKFLOW_OMEGAS), kmesh=WORKFLOW_KMESH)
+    out["workflow_values"] = res["values"]
+    meta = {k: res[k] for k in ("eta_records", "omega_failures", "n_rejected_total", "summary")}
+    out["workflow_meta"] = np.array(json.dumps(meta, default=lambda o: list(o) if isinstance(o, tuple) else o))
+    np.savez_compressed(out_dir / "interface.npz", **out)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference/src")
-    ap.add_argument("--only", choices=["thermal", "green", "workflow"], default=None,
+    ap.add_argument("--only", choices=["thermal", "green", "workflow", "interface"], default=None,
                     help="write one fixture file only")
     args = ap.parse_args()
     sys.path.insert(0, args.ref)
@@ -172,6 +247,10 @@ def main() -> None:
     if args.only == "workflow":
         workflow(OUT)
         print("wrote workflow.npz")
+        return
+    if args.only == "interface":
+        interface(OUT)
+        print("wrote interface.npz")
         return
     import negfpy.core as R
     from negfpy.core.types import Device1D, LeadBlocks
