@@ -208,6 +208,56 @@ def _systems_over_k(omega, device, lead_left, lead_right, kpoints, eta, eta_devi
             for k in kpoints]
 
 
+class _KBatch:
+    """All k points of one per-omega call, stacked on the GPU once.
+
+    The blocks of every k come from the GPU builder when the system is a
+    material or interface-contact set-up of one parameter set
+    (``spectrum._material_fast_path``); otherwise from the per-k host
+    builders.  The first k always goes through ``point_system``, which
+    validates the call and fixes negfpy's omega-scale and device-eta rules
+    (``core/negf.py:163-190``).  ``run`` solves any subset of the k points at
+    one ladder eta against the same stack.
+    """
+
+    def __init__(self, omega, device, lead_left, lead_right, kpoints, eta_device, device_to_lead_left,
+                 device_to_lead_right, contact_left_indices, contact_right_indices, omega_scale):
+        from .spectrum import _material_fast_path
+
+        self.K = len(kpoints)
+        fast = _material_fast_path(device, lead_left, lead_right, device_to_lead_left, device_to_lead_right,
+                                   contact_left_indices, contact_right_indices, omega_scale)
+        ks = list(kpoints) if fast is None else list(kpoints[:1])
+        systems = _prepare_ladder_systems(omega, device, lead_left, lead_right, ks, eta_device,
+                                          device_to_lead_left, device_to_lead_right, contact_left_indices,
+                                          contact_right_indices, omega_scale)
+        if fast is None:
+            self.sys, _ = stack_systems(systems)
+        else:
+            from .kspace import interface_system, stacked_system
+
+            build = interface_system if fast[0] == "interface" else stacked_system
+            self.sys = build(fast[1], fast[2], [() if k is None else k for k in kpoints])
+        s0 = systems[0]
+        self.omega, self.scale, self.eta_dev_for = s0["omega"], s0["scale"], s0["_eta_dev_for"]
+
+    def run(self, eta: float, idx: list) -> tuple[np.ndarray, np.ndarray]:
+        """T and status of the k points ``idx`` at lead eta ``eta`` (before the
+        omega scale).  A negative device eta is negfpy's ValueError, i.e. an
+        "exception" rejection (status -1, T NaN)."""
+        ed = self.eta_dev_for(eta)
+        if ed < 0.0:
+            return np.full(len(idx), np.nan), np.full(len(idx), -1, dtype=np.int32)
+        dev = _lib.require_cuda()
+        P = len(idx)
+        om = torch.full((P,), float(self.omega), dtype=torch.float64, device=dev)
+        et = torch.full((P,), float(eta) / self.scale, dtype=torch.float64, device=dev)
+        edt = torch.full((P,), float(ed), dtype=torch.float64, device=dev)
+        ki = torch.tensor(list(idx), dtype=torch.int32, device=dev)
+        r = self.sys.transmission(om, ki, et, edt)
+        return r["T"].cpu().numpy(), r["status"].cpu().numpy()
+
+
 def transmission_kavg(omega: float, device, lead_left, lead_right, kpoints: list, eta: float = 1e-8,
                       eta_device: float | None = None, device_to_lead_left=None, device_to_lead_right=None,
                       contact_left_indices=None, contact_right_indices=None, surface_gf_method: str = "sancho_rubio",
@@ -216,9 +266,11 @@ def transmission_kavg(omega: float, device, lead_left, lead_right, kpoints: list
     if len(kpoints) == 0:
         raise ValueError("kpoints must contain at least one k-point.")
     check_method(surface_gf_method)
-    systems = _systems_over_k(omega, device, lead_left, lead_right, kpoints, eta, eta_device, device_to_lead_left,
-                              device_to_lead_right, contact_left_indices, contact_right_indices, omega_scale)
-    t, st = _run_points(systems)
+    if float(eta if eta_device is None else eta_device) < 0.0:
+        raise ValueError("eta_device must be non-negative.")
+    kb = _KBatch(omega, device, lead_left, lead_right, kpoints, eta_device, device_to_lead_left,
+                 device_to_lead_right, contact_left_indices, contact_right_indices, omega_scale)
+    t, st = kb.run(float(eta), list(range(kb.K)))
     for s in st:
         raise_for_status(int(s))
     return float(np.mean(t))
@@ -251,20 +303,6 @@ def _classify(t, st, max_allowed, nonneg_tol):
     return None
 
 
-def _ladder_run(systems, eta, idx):
-    """Run the k points ``idx`` at ladder broadening ``eta``.
-
-    Lead eta and device eta follow negfpy ``negf.py:163-181``: eta_device
-    defaults to eta, and both are divided by omega_scale.  A negative
-    device eta is the reference's ValueError, i.e. an "exception" rejection.
-    """
-    sub = [systems[i] for i in idx]
-    ed = [s["_eta_dev_for"](eta) for s in sub]
-    if any(e < 0.0 for e in ed):
-        return np.full(len(sub), np.nan), np.full(len(sub), -1, dtype=np.int32)
-    return _run_points(sub, etas=[eta / s["scale"] for s in sub], eta_devs=ed)
-
-
 def _prepare_ladder_systems(omega, device, lead_left, lead_right, kpoints, eta_device, device_to_lead_left,
                             device_to_lead_right, contact_left_indices, contact_right_indices, omega_scale):
     systems = _systems_over_k(omega, device, lead_left, lead_right, kpoints, 1.0, eta_device, device_to_lead_left,
@@ -295,21 +333,18 @@ def transmission_kavg_adaptive(omega: float, device, lead_left, lead_right, kpoi
     """
     _check_adaptive_args(kpoints, eta_values, min_success_fraction, nonnegative_tolerance, max_channel_factor)
     check_method(surface_gf_method)
-    systems = _prepare_ladder_systems(omega, device, lead_left, lead_right, kpoints, eta_device,
-                                      device_to_lead_left, device_to_lead_right, contact_left_indices,
-                                      contact_right_indices, omega_scale)
+    kb = _KBatch(omega, device, lead_left, lead_right, kpoints, eta_device, device_to_lead_left,
+                 device_to_lead_right, contact_left_indices, contact_right_indices, omega_scale)
     K = len(kpoints)
-    max_allowed = [None] * K
-    if max_channel_factor is not None:
-        for i, k in enumerate(kpoints):
-            max_allowed[i] = float(max_channel_factor) * float(resolve_lead_blocks(lead_left, k).d00.shape[0])
+    # one call shares the lead order over its k points (stack_systems checks it)
+    max_allowed = [None if max_channel_factor is None else float(max_channel_factor) * float(kb.sys.nl)] * K
     accepted: dict[int, tuple[float, float]] = {}
     attempts: list[tuple[int, int, dict]] = []
     pending = list(range(K))
     for ei, eta in enumerate(eta_values):
         if not pending:
             break
-        t, st = _ladder_run(systems, float(eta), pending)
+        t, st = kb.run(float(eta), pending)
         nxt = []
         for j, ki in enumerate(pending):
             reason = _classify(t[j], st[j], max_allowed[ki], nonnegative_tolerance)
@@ -359,17 +394,14 @@ def transmission_kavg_adaptive_global_eta(omega: float, device, lead_left, lead_
     """One eta per omega (negfpy ``core/negf.py:546-688``): all k per rung in one batch."""
     _check_adaptive_args(kpoints, eta_values, min_success_fraction, nonnegative_tolerance, max_channel_factor)
     check_method(surface_gf_method)
-    systems = _prepare_ladder_systems(omega, device, lead_left, lead_right, kpoints, eta_device,
-                                      device_to_lead_left, device_to_lead_right, contact_left_indices,
-                                      contact_right_indices, omega_scale)
+    kb = _KBatch(omega, device, lead_left, lead_right, kpoints, eta_device, device_to_lead_left,
+                 device_to_lead_right, contact_left_indices, contact_right_indices, omega_scale)
     K = len(kpoints)
-    max_allowed = [None] * K
-    if max_channel_factor is not None:
-        for i, k in enumerate(kpoints):
-            max_allowed[i] = float(max_channel_factor) * float(resolve_lead_blocks(lead_left, k).d00.shape[0])
+    # one call shares the lead order over its k points (stack_systems checks it)
+    max_allowed = [None if max_channel_factor is None else float(max_channel_factor) * float(kb.sys.nl)] * K
     rejected_all: list = []
     for eta in eta_values:
-        t, st = _ladder_run(systems, float(eta), list(range(K)))
+        t, st = kb.run(float(eta), list(range(K)))
         vals = []
         for ki in range(K):
             reason = _classify(t[ki], st[ki], max_allowed[ki], nonnegative_tolerance)

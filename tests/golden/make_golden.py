@@ -220,6 +220,21 @@ def interface(out_dir: Path) -> None:
     prm = interface_params("slab", MaterialKspaceParams)
     ll, lr, vdl_l, vdl_r = ifc_bulk._build_interface_contacts(prm)
     dev = material_kspace_device(n_layers=4, params=prm)
+    # the per-omega k averages and eta ladders through the same contacts
+    kp = INTERFACE_KPOINTS["slab"]
+    w = float(out["slab_omegas"][1])
+    wmax2 = (w / INTERFACE_FRACTIONS[1]) ** 2
+    kw = dict(device_to_lead_left=vdl_l, device_to_lead_right=vdl_r)
+    ladder = tuple(f * wmax2 for f in (1e-7, 1e-5, 1e-3))
+    out["kavg"] = R.transmission_kavg(w, dev, ll, lr, kpoints=kp, eta=float(out["slab_eta"]), **kw)
+    val, info = R.transmission_kavg_adaptive(w, dev, ll, lr, kpoints=kp, eta_values=ladder, max_channel_factor=0.2,
+                                             collect_rejected=True, **kw)
+    out["adaptive_value"], out["adaptive_info"] = val, np.array(json.dumps(info, default=list))
+    val, info = R.transmission_kavg_adaptive_global_eta(w, dev, ll, lr, kpoints=kp, eta_values=ladder,
+                                                        max_channel_factor=0.2, min_success_fraction=0.3,
+                                                        collect_rejected=True, **kw)
+    out["global_value"], out["global_info"] = val, np.array(json.dumps(info, default=list))
+    out["ladder"] = np.array(ladder)
     res = ifc_bulk._run_transmission(WORKFLOW_CFGS["adaptive"], device=dev, lead_left=ll, lead_right=lr,
                                      device_to_lead_left=vdl_l, device_to_lead_right=vdl_r,
                                      omegas=np.array(WORKFLOW_OMEGAS), kmesh=WORKFLOW_KMESH)

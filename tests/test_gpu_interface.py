@@ -88,3 +88,25 @@ def test_workflow_with_interface_contacts_matches_negfpy(fix):
     ours = _norm({k: res[k] for k in ("eta_records", "omega_failures", "n_rejected_total", "summary")})
     ours["summary"]["parallel"]["workers"] = meta["summary"]["parallel"]["workers"]  # host core count differs
     _close(ours, meta, 1e-12)
+
+
+def test_per_omega_ladders_match_negfpy(fix):
+    """transmission_kavg and both eta ladders through the contacts (all k
+    blocks built on the GPU once per call) against negfpy's values and info
+    dictionaries, rejected records included."""
+    prm = params_of(fix, "slab")
+    ll, lr, vdl_l, vdl_r = interface_contacts(prm)
+    dev = material_kspace_device(4, prm)
+    kp = kpoints_of("slab")
+    w = float(fix["slab_omegas"][1])
+    kw = dict(device_to_lead_left=vdl_l, device_to_lead_right=vdl_r)
+    ladder = tuple(float(x) for x in fix["ladder"])
+    t = nb.transmission_kavg(w, dev, ll, lr, kpoints=kp, eta=float(fix["slab_eta"]), **kw)
+    assert abs(t - float(fix["kavg"])) <= 1e-10 * max(1.0, abs(float(fix["kavg"])))
+    for key, fn, extra in (("adaptive", nb.transmission_kavg_adaptive, {}),
+                           ("global", nb.transmission_kavg_adaptive_global_eta, {"min_success_fraction": 0.3})):
+        val, info = fn(w, dev, ll, lr, kpoints=kp, eta_values=ladder, max_channel_factor=0.2, collect_rejected=True,
+                       **kw, **extra)
+        ref = float(fix[key + "_value"])
+        assert abs(val - ref) <= 1e-10 * max(1.0, abs(ref)), key
+        _close(_norm(info), json.loads(str(fix[key + "_info"])), 1e-10)
