@@ -220,7 +220,7 @@ def test_bulk_n96_matches_reference(golden_bulk):
     assert np.max(np.abs(gs - g["g"])) <= 1e-10 * np.max(np.abs(g["g"]))
 
 
-@pytest.mark.parametrize("n", [49, 64, 96, 150, 192])
+@pytest.mark.parametrize("n", [49, 64, 96, 150, 192, 256])
 def test_inversion_large_orders_against_numpy(n):
     rng = np.random.default_rng(n)
     d00 = rng.normal(size=(n, n)) + 1j * rng.normal(size=(n, n))
@@ -230,6 +230,31 @@ def test_inversion_large_orders_against_numpy(n):
     g = nb.surface_gf(0.7, d00, np.zeros((n, n)), eta=0.01)
     err = np.max(np.abs(g - ref)) / np.max(np.abs(ref))
     assert err <= 1e-12 * np.linalg.cond(m), err
+
+
+def test_largest_block_order_transmission_vs_oracle():
+    """n = 255 (85 atoms x 3 DOF, padded to the largest supported order 256):
+    T through the global-workspace kernels against the oracle at three
+    (omega, k) points, and order 257 is rejected."""
+    from negfpy_b200.models import material_kspace_device, material_kspace_lead
+
+    p = W.spring_network(4, ny=5, nz=17, periodic_y=True, periodic_z=False)
+    assert p.ndof == 255
+    wmax = W.estimate_omega_max(p, nk=4)
+    eta = 1e-5 * wmax * wmax
+    kp = [(0.4,), (-2.1,)]
+    lead, dev = material_kspace_lead(p), material_kspace_device(3, p)
+    om = np.array([0.23, 0.61]) * wmax
+    r = nb.transmission_grid(om, kp, dev, lead, lead, eta=eta)
+    assert np.all(r["status"] == 0)
+    for wi, ki in ((0, 0), (1, 0), (1, 1)):
+        d = dev.device(kp[ki])
+        lb = lead.blocks(kp[ki])
+        ref = O.transmission_point(float(om[wi]), list(d.onsite_blocks), list(d.coupling_blocks), lb, lb, eta=eta)
+        assert abs(r["T"][wi, ki] - ref) <= TOL_T * max(1.0, abs(ref)), (wi, ki, r["T"][wi, ki], ref)
+    big = np.eye(257, dtype=complex)
+    with pytest.raises(RuntimeError, match="block order 257 is not supported"):
+        nb.surface_gf(0.5, big, np.zeros_like(big), eta=0.01)
 
 
 def test_mixed_orders_heterojunction_vs_oracle():
