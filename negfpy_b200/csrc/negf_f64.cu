@@ -407,6 +407,9 @@ __device__ int gj_invert(double2* X, double2* Y, double2* Z, int n, const Lane& 
       unsigned nk = 0u;
 #pragma unroll
       for (int q = 0; q < PPT; ++q) {
+        // Slots past the panel are whole warps (PE and NTH are multiples of
+        // 32), so this skips their arithmetic without divergence.
+        if (!pin[q]) continue;
         const int r = pr_[q], c = pc_[q];
         const bool isp = (r == pr);
         used[q] = used[q] || isp;
@@ -415,10 +418,8 @@ __device__ int gj_invert(double2* X, double2* Y, double2* Z, int n, const Lane& 
         const double2 m = (c == j) ? lam : mv[q];
         double2 v = cneg(cmul(b, m));
         if (!isp && c != j) cfma(v, ps, av[q]);
-        if (pin[q]) {
-          Pn[pidx(r, c)] = v;
-          if (c == j + 1 && !used[q] && r >= k0 && r < n) nk = max(nk, pivot_key(v, r));
-        }
+        Pn[pidx(r, c)] = v;
+        if (c == j + 1 && !used[q] && r >= k0 && r < n) nk = max(nk, pivot_key(v, r));
       }
       lam = cmul(lam, ps);
       if (j + 1 < jmax) {
