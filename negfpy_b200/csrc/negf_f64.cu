@@ -339,15 +339,19 @@ __device__ int gj_invert(double2* X, double2* Y, double2* Z, int n, const Lane& 
   int cols[4], scol[4];
 #pragma unroll
   for (int ci = 0; ci < 4; ++ci) cols[ci] = scol[ci] = L.n0 + 8 * (ci >> 1) + 2 * L.t + (ci & 1);
-  // panel elements owned by this thread
+  // Panel elements owned by this thread: element e = tid + q NTH.  A partly
+  // filled last slot (n = 48: 96 elements) goes to warps 1, 2, 3 rather
+  // than 0, 1, 2, so that each of the SM's four sub-partitions (warp index
+  // mod 4) carries the same number of slots.
   int pr_[PPT], pc_[PPT];
   bool pin[PPT];
 #pragma unroll
   for (int q = 0; q < PPT; ++q) {
-    const int e = tid + q * NTH;
-    pin[q] = e < PE;
+    const bool partial = (q + 1) * NTH > PE;
+    const int e = partial ? tid - 32 + q * NTH : tid + q * NTH;
+    pin[q] = partial ? (tid >= 32 && e < PE) : true;
     pr_[q] = pin[q] ? (e >> 3) : 0;
-    pc_[q] = e & 7;
+    pc_[q] = (pin[q] ? e : 0) & 7;
   }
 
   for (int k0 = 0; k0 < n; k0 += 8) {
