@@ -157,8 +157,10 @@ __device__ __forceinline__ void cmma(double (&cr)[4], double (&ci)[4], const dou
 }
 
 // c = op(A) op(B) over the first kch chunks of 8 (the rest is zero padding).
+// jm: warp-uniform mask of the two 16 x 8 halves (j) to compute.
 template <int NP, bool AC, bool BC>
-__device__ __forceinline__ void cmm(CAcc& c, const double2* A, const double2* B, int kch, const Lane& L) {
+__device__ __forceinline__ void cmm(CAcc& c, const double2* A, const double2* B, int kch, const Lane& L,
+                                    int jm = 3) {
   int ab[4], bb[2][2];
   a_bases<NP, AC>(L, ab);
   b_bases<NP, BC>(L, bb);
@@ -168,6 +170,7 @@ __device__ __forceinline__ void cmm(CAcc& c, const double2* A, const double2* B,
     load_a<NP, AC>(A, ab, kc * 8, ar, ai);
 #pragma unroll
     for (int j = 0; j < 2; ++j) {
+      if (!((jm >> j) & 1)) continue;
       double br[2], bi[2];
       load_b<NP, BC>(B, bb[j], kc * 8, br, bi);
       cmma(c.re[j], c.im[j], ar, ai, br, bi);
@@ -177,7 +180,7 @@ __device__ __forceinline__ void cmm(CAcc& c, const double2* A, const double2* B,
 // c1 = A1 B, c2 = A2 B.
 template <int NP>
 __device__ __forceinline__ void cmm2b(CAcc& c1, CAcc& c2, const double2* A1, const double2* A2, const double2* B,
-                                      int kch, const Lane& L) {
+                                      int kch, const Lane& L, int jm = 3) {
   int ab[4], bb[2][2];
   a_bases<NP, false>(L, ab);
   b_bases<NP, false>(L, bb);
@@ -189,6 +192,7 @@ __device__ __forceinline__ void cmm2b(CAcc& c1, CAcc& c2, const double2* A1, con
     load_a<NP, false>(A2, ab, kc * 8, a2r, a2i);
 #pragma unroll
     for (int j = 0; j < 2; ++j) {
+      if (!((jm >> j) & 1)) continue;
       double br[2], bi[2];
       load_b<NP, false>(B, bb[j], kc * 8, br, bi);
       cmma(c1.re[j], c1.im[j], a1r, a1i, br, bi);
@@ -198,12 +202,35 @@ __device__ __forceinline__ void cmm2b(CAcc& c1, CAcc& c2, const double2* A1, con
 }
 
 template <int NP>
-__device__ __forceinline__ void store_acc(double2* S, const CAcc& c, const Lane& L) {
+__device__ __forceinline__ void store_acc(double2* S, const CAcc& c, const Lane& L, int jm = 3) {
 #pragma unroll
   for (int j = 0; j < 2; ++j)
 #pragma unroll
-    for (int q = 0; q < 4; ++q) S[sidx<NP>(own_r(L, q), own_c(L, j, q))] = c.get(j, q);
+    for (int q = 0; q < 4; ++q)
+      if ((jm >> j) & 1) S[sidx<NP>(own_r(L, q), own_c(L, j, q))] = c.get(j, q);
 }
+
+// Work split of the products between the SM's four sub-partitions (warp
+// index mod 4).  With 9 warps (NP = 48) sub-partition 0 runs warps 0, 4
+// and 8; the right half (j = 1) of warp 8's tile is done by warp 3
+// instead, so the sub-partitions carry 5, 4, 4 and 5 halves, not 6, 4, 4, 4.
+// The moved half keeps its arithmetic; its eps lives in shared memory
+// (lane-private, epsx[q * 32 + lane]) and is owned by warp 3.
+template <int NP>
+struct Split {
+  static constexpr bool on = Geo<NP>::NW == 9;
+  int jm;      // halves of the own tile this warp computes
+  bool extra;  // this warp also computes the moved half
+  Lane Lx;     // geometry of the moved half's tile (use with j = 1)
+  __device__ __forceinline__ explicit Split(const Lane& L) {
+    const int w = threadIdx.x >> 5;
+    jm = (on && w == 8) ? 1 : 3;
+    extra = on && w == 3;
+    Lx = L;
+    Lx.m0 = 32;
+    Lx.n0 = 32;
+  }
+};
 
 // Global nr x nc row-major matrix -> padded shared buffer (zeros outside).
 template <int NP>
@@ -541,6 +568,7 @@ __global__ void __launch_bounds__(Geo<NP>::NTH, 1) sr_f64_kernel(SrArgs a) {
   double2* pes = f2 + MAT;
   const GJShared gsh = carve_gj<NP>(reinterpret_cast<unsigned char*>(pes + MAT));
   double* red = carve_red<NP>(pes + MAT);
+  double2* epsx = reinterpret_cast<double2*>(red + 40);  // eps of the moved half (Split)
 
   const int p = blockIdx.x;
   if (p >= a.batch) return;
@@ -555,6 +583,8 @@ __global__ void __launch_bounds__(Geo<NP>::NTH, 1) sr_f64_kernel(SrArgs a) {
   const double w = a.omega[p];
   const double2 z = z_of(w, a.eta[p]);
 
+  const Split<NP> sp(L);
+  const int lane = tid & 31;
   double2 eps[8];
 #pragma unroll
   for (int j = 0; j < 2; ++j)
@@ -563,8 +593,17 @@ __global__ void __launch_bounds__(Geo<NP>::NTH, 1) sr_f64_kernel(SrArgs a) {
       const int r = own_r(L, q), c = own_c(L, j, q);
       const double2 e = (r < n && c < n) ? h00[r * n + c] : make_double2(0.0, 0.0);
       eps[j * 4 + q] = e;
+      if ((sp.jm >> j) & 1) pes[sidx<NP>(r, c)] = e;
+    }
+  if (sp.extra) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int r = own_r(sp.Lx, q), c = own_c(sp.Lx, 1, q);
+      const double2 e = (r < n && c < n) ? h00[r * n + c] : make_double2(0.0, 0.0);
+      epsx[q * 32 + lane] = e;
       pes[sidx<NP>(r, c)] = e;
     }
+  }
   for (int idx = tid; idx < NP * NP; idx += G::NTH) {
     const int r = idx / NP, c = idx - r * NP;
     const bool in = r < n && c < n;
@@ -584,64 +623,123 @@ __global__ void __launch_bounds__(Geo<NP>::NTH, 1) sr_f64_kernel(SrArgs a) {
     for (int j = 0; j < 2; ++j)
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
+        if (!((sp.jm >> j) & 1)) continue;
         const int r = own_r(L, q), c = own_c(L, j, q);
         double2 v;
         if (r < n && c < n) v = (r == c) ? csub(z, eps[j * 4 + q]) : cneg(eps[j * 4 + q]);
         else v = make_double2(r == c ? 1.0 : 0.0, 0.0);
         f0[sidx<NP>(r, c)] = v;
       }
+    if (sp.extra) {
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int r = own_r(sp.Lx, q), c = own_c(sp.Lx, 1, q);
+        const double2 e = epsx[q * 32 + lane];
+        double2 v;
+        if (r < n && c < n) v = (r == c) ? csub(z, e) : cneg(e);
+        else v = make_double2(r == c ? 1.0 : 0.0, 0.0);
+        f0[sidx<NP>(r, c)] = v;
+      }
+    }
     __syncthreads();
     status = gj_invert<NP>(f0, f1, f2, n, L, gsh, &pg);
     if (status != kOk) break;
     double2* pag = (pg == f0) ? f1 : f0;  // the inversion's other buffer
     double2* pbg = f2;
     // alpha g, beta g
-    cmm2b<NP>(c1, c2, pa, pb, pg, kch, L);
-    store_acc<NP>(pag, c1, L);
-    store_acc<NP>(pbg, c2, L);
+    cmm2b<NP>(c1, c2, pa, pb, pg, kch, L, sp.jm);
+    store_acc<NP>(pag, c1, L, sp.jm);
+    store_acc<NP>(pbg, c2, L, sp.jm);
+    if (sp.extra) {
+      cmm2b<NP>(c1, c2, pa, pb, pg, kch, sp.Lx, 2);
+      store_acc<NP>(pag, c1, sp.Lx, 2);
+      store_acc<NP>(pbg, c2, sp.Lx, 2);
+    }
     __syncthreads();
     // eps_s += (alpha g) beta ; eps += (alpha g) beta + (beta g) alpha
     int bad = 0;
-    cmm<NP, false, false>(c1, pag, pb, kch, L);
+    cmm<NP, false, false>(c1, pag, pb, kch, L, sp.jm);
 #pragma unroll
     for (int j = 0; j < 2; ++j)
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
+        if (!((sp.jm >> j) & 1)) continue;
         const int e = sidx<NP>(own_r(L, q), own_c(L, j, q));
         const double2 es = cadd(pes[e], c1.get(j, q));
         pes[e] = es;
         eps[j * 4 + q] = cadd(eps[j * 4 + q], c1.get(j, q));
         bad |= !cfinite(es);
       }
-    cmm<NP, false, false>(c1, pbg, pa, kch, L);
+    if (sp.extra) {
+      cmm<NP, false, false>(c1, pag, pb, kch, sp.Lx, 2);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int e = sidx<NP>(own_r(sp.Lx, q), own_c(sp.Lx, 1, q));
+        const double2 es = cadd(pes[e], c1.get(1, q));
+        pes[e] = es;
+        epsx[q * 32 + lane] = cadd(epsx[q * 32 + lane], c1.get(1, q));
+        bad |= !cfinite(es);
+      }
+    }
+    cmm<NP, false, false>(c1, pbg, pa, kch, L, sp.jm);
 #pragma unroll
     for (int j = 0; j < 2; ++j)
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
+        if (!((sp.jm >> j) & 1)) continue;
         eps[j * 4 + q] = cadd(eps[j * 4 + q], c1.get(j, q));
         bad |= !cfinite(eps[j * 4 + q]);
       }
+    if (sp.extra) {
+      cmm<NP, false, false>(c1, pbg, pa, kch, sp.Lx, 2);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const double2 e = cadd(epsx[q * 32 + lane], c1.get(1, q));
+        epsx[q * 32 + lane] = e;
+        bad |= !cfinite(e);
+      }
+    }
     // alpha' = (alpha g) alpha into the free g buffer ; beta' = (beta g) beta
     double e2 = 0.0;
-    cmm<NP, false, false>(c1, pag, pa, kch, L);
+    cmm<NP, false, false>(c1, pag, pa, kch, L, sp.jm);
 #pragma unroll
     for (int j = 0; j < 2; ++j)
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
+        if (!((sp.jm >> j) & 1)) continue;
         bad |= !cfinite(c1.get(j, q));
         e2 = fmax(e2, cabs2(c1.get(j, q)));
       }
-    store_acc<NP>(pg, c1, L);
-    cmm<NP, false, false>(c1, pbg, pb, kch, L);
+    store_acc<NP>(pg, c1, L, sp.jm);
+    if (sp.extra) {
+      cmm<NP, false, false>(c1, pag, pa, kch, sp.Lx, 2);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        bad |= !cfinite(c1.get(1, q));
+        e2 = fmax(e2, cabs2(c1.get(1, q)));
+      }
+      store_acc<NP>(pg, c1, sp.Lx, 2);
+    }
+    cmm<NP, false, false>(c1, pbg, pb, kch, L, sp.jm);
 #pragma unroll
     for (int j = 0; j < 2; ++j)
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
+        if (!((sp.jm >> j) & 1)) continue;
         bad |= !cfinite(c1.get(j, q));
         e2 = fmax(e2, cabs2(c1.get(j, q)));
       }
+    if (sp.extra) {  // beta' of the moved half waits in c2 for the barrier
+      cmm<NP, false, false>(c2, pbg, pb, kch, sp.Lx, 2);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        bad |= !cfinite(c2.get(1, q));
+        e2 = fmax(e2, cabs2(c2.get(1, q)));
+      }
+    }
     __syncthreads();  // every read of alpha and beta is done
-    store_acc<NP>(pb, c1, L);
+    store_acc<NP>(pb, c1, L, sp.jm);
+    if (sp.extra) store_acc<NP>(pb, c2, sp.Lx, 2);
     f0 = pa;  // old alpha buffer is free
     f1 = pag;
     f2 = pbg;
@@ -655,6 +753,7 @@ __global__ void __launch_bounds__(Geo<NP>::NTH, 1) sr_f64_kernel(SrArgs a) {
     it = a.maxiter;
   }
   if (status == kOk) {
+    // every element of eps_s is in shared memory: each thread builds its own tile
 #pragma unroll
     for (int j = 0; j < 2; ++j)
 #pragma unroll
@@ -1108,7 +1207,9 @@ __global__ void heat_current_kernel(const double* __restrict__ om, const double*
 template <int NP>
 static size_t smem_bytes() { return (size_t)5 * Geo<NP>::MAT * 16 + tail_bytes<NP>(); }
 template <int NP>
-static size_t sr_smem_bytes() { return (size_t)6 * Geo<NP>::MAT * 16 + tail_bytes<NP>(); }
+static size_t sr_smem_bytes() {
+  return (size_t)6 * Geo<NP>::MAT * 16 + tail_bytes<NP>() + (Split<NP>::on ? 4 * 32 * 16 : 0);  // + epsx
+}
 
 // Last launch failure of this host thread (read by the C-ABI layer).
 thread_local char g_launch_err[256] = "";
