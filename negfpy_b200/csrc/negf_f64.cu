@@ -813,6 +813,10 @@ __global__ void __launch_bounds__(Geo<NP>::NTH, 1) rgf_f64_kernel(RgfArgs a) {
   const int kch = (n + 7) >> 3;
   const int tid = threadIdx.x;
   const Lane Ln = lane_geo<NP>();
+  // Per-layer products split between sub-partitions as in the decimation
+  // (Split); the once-per-point self-energies and trace keep whole tiles, so
+  // the trace's block sum adds the same per-thread terms as before.
+  const Split<NP> sp(Ln);
   double2* sigL = a.sigma_ws + (long long)blockIdx.x * 2 * n * n;
   double2* sigR = sigL + (long long)n * n;
   CAcc c1, c2;
@@ -895,37 +899,51 @@ __global__ void __launch_bounds__(Geo<NP>::NTH, 1) rgf_f64_kernel(RgfArgs a) {
         load_mat<NP>(pc, C + (long long)(l - 1) * a.c_ls, n, n);
         __syncthreads();
         // W = g_{l-1} C, U = G_{0,l-1} C
-        cmm2b<NP>(c1, c2, pg, bG0, pc, kch, Ln);
-        store_acc<NP>(bW, c1, Ln);
-        store_acc<NP>(bU, c2, Ln);
+        cmm2b<NP>(c1, c2, pg, bG0, pc, kch, Ln, sp.jm);
+        store_acc<NP>(bW, c1, Ln, sp.jm);
+        store_acc<NP>(bU, c2, Ln, sp.jm);
+        if (sp.extra) {
+          cmm2b<NP>(c1, c2, pg, bG0, pc, kch, sp.Lx, 2);
+          store_acc<NP>(bW, c1, sp.Lx, 2);
+          store_acc<NP>(bU, c2, sp.Lx, 2);
+        }
         __syncthreads();
         // M = z - D_l - C^H W [- Sigma_R on the last layer] into the old g buffer
-        cmm<NP, true, false>(c1, pc, bW, kch, Ln);
         const double2* Dl = D + (long long)l * a.d_ls;
         const bool last = (l == L - 1);
+        auto form_m = [&](const Lane& Lm, int jm) {
+          cmm<NP, true, false>(c1, pc, bW, kch, Lm, jm);
 #pragma unroll
-        for (int j = 0; j < 2; ++j)
+          for (int j = 0; j < 2; ++j)
 #pragma unroll
-          for (int q = 0; q < 4; ++q) {
-            const int r = own_r(Ln, q), c = own_c(Ln, j, q);
-            double2 v;
-            if (r < n && c < n) {
-              v = csub(cneg(Dl[r * n + c]), c1.get(j, q));
-              if (last) v = csub(v, sigR[r * n + c]);
-              if (r == c) v = cadd(v, z);
-            } else {
-              v = make_double2(r == c ? 1.0 : 0.0, 0.0);
+            for (int q = 0; q < 4; ++q) {
+              if (!((jm >> j) & 1)) continue;
+              const int r = own_r(Lm, q), c = own_c(Lm, j, q);
+              double2 v;
+              if (r < n && c < n) {
+                v = csub(cneg(Dl[r * n + c]), c1.get(j, q));
+                if (last) v = csub(v, sigR[r * n + c]);
+                if (r == c) v = cadd(v, z);
+              } else {
+                v = make_double2(r == c ? 1.0 : 0.0, 0.0);
+              }
+              pg[sidx<NP>(r, c)] = v;
             }
-            pg[sidx<NP>(r, c)] = v;
-          }
+        };
+        form_m(Ln, sp.jm);
+        if (sp.extra) form_m(sp.Lx, 2);
         __syncthreads();  // C is dead once M is formed: pc becomes the second inversion buffer
         status = gj_invert<NP>(pg, pc, bW, n, Ln, gsh, &inv);
         if (status != kOk) break;
         pc = (inv == pg) ? pc : pg;
         pg = inv;
         // G_{0,l} = U g_l
-        cmm<NP, false, false>(c1, bU, pg, kch, Ln);
-        store_acc<NP>(bG0, c1, Ln);
+        cmm<NP, false, false>(c1, bU, pg, kch, Ln, sp.jm);
+        store_acc<NP>(bG0, c1, Ln, sp.jm);
+        if (sp.extra) {
+          cmm<NP, false, false>(c1, bU, pg, kch, sp.Lx, 2);
+          store_acc<NP>(bG0, c1, sp.Lx, 2);
+        }
         __syncthreads();
       }
     }
