@@ -41,8 +41,12 @@ __device__ __forceinline__ double2 z_of(double w, double e) {
 template <int NP>
 struct Geo {
   static constexpr int T = NP / 16;     // 16-row tiles per side
-  static constexpr int NW = T * T;      // warps, one 16 x 16 region each
-  static constexpr int NTH = 32 * NW;   // threads
+  static constexpr int NW = T * T;      // tile warps, one 16 x 16 region each
+  // Warps per block: a multiple of the SM's 4 sub-partitions.  At NP = 48
+  // the 3 warps beyond the 9 tile warps own no tile; they take part in the
+  // Gauss-Jordan panel (one element per thread) and its bookkeeping.
+  static constexpr int NWB = (NW % 4 == 0 || NW == 1) ? NW : (NW + 3) / 4 * 4;
+  static constexpr int NTH = 32 * NWB;  // threads
   static constexpr int MAT = NP * NP;   // complex elements per matrix buffer
 };
 
@@ -61,9 +65,12 @@ __device__ __forceinline__ int sidx(int r, int c) { return r * NP + (c ^ swz(r))
 struct Lane {
   int g, t, m0, n0;
 };
+// Warps without a tile get tile 0's geometry, so that any fragment address
+// they form stays in range; tile-owned work masks them out (Split::jt).
 template <int NP>
 __device__ __forceinline__ Lane lane_geo() {
-  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  const int w0 = threadIdx.x >> 5, l = threadIdx.x & 31;
+  const int w = w0 < Geo<NP>::NW ? w0 : 0;
   Lane L;
   L.g = l >> 2;
   L.t = l & 3;
@@ -165,6 +172,7 @@ __device__ __forceinline__ void cmm(CAcc& c, const double2* A, const double2* B,
   a_bases<NP, AC>(L, ab);
   b_bases<NP, BC>(L, bb);
   c.zero();
+  if (!jm) return;
   for (int kc = 0; kc < kch; ++kc) {
     double ar[4], ai[4];
     load_a<NP, AC>(A, ab, kc * 8, ar, ai);
@@ -186,6 +194,7 @@ __device__ __forceinline__ void cmm2b(CAcc& c1, CAcc& c2, const double2* A1, con
   b_bases<NP, false>(L, bb);
   c1.zero();
   c2.zero();
+  if (!jm) return;
   for (int kc = 0; kc < kch; ++kc) {
     double a1r[4], a1i[4], a2r[4], a2i[4];
     load_a<NP, false>(A1, ab, kc * 8, a1r, a1i);
@@ -219,13 +228,18 @@ __device__ __forceinline__ void store_acc(double2* S, const CAcc& c, const Lane&
 template <int NP>
 struct Split {
   static constexpr bool on = Geo<NP>::NW == 9;
-  int jm;      // halves of the own tile this warp computes
+  // The moved half goes to a warp of sub-partition 3: the last warp, which
+  // owns no tile when the block has more warps than tiles, else warp 3.
+  static constexpr int kHelper = Geo<NP>::NWB > Geo<NP>::NW ? Geo<NP>::NWB - 1 : 3;
+  int jt;      // halves of the own tile, 0 for warps without a tile
+  int jm;      // halves of the own tile this warp computes in the split products
   bool extra;  // this warp also computes the moved half
   Lane Lx;     // geometry of the moved half's tile (use with j = 1)
   __device__ __forceinline__ explicit Split(const Lane& L) {
     const int w = threadIdx.x >> 5;
-    jm = (on && w == 8) ? 1 : 3;
-    extra = on && w == 3;
+    jt = w < Geo<NP>::NW ? 3 : 0;
+    jm = (on && w == 8) ? 1 : jt;
+    extra = on && w == kHelper;
     Lx = L;
     Lx.m0 = 32;
     Lx.n0 = 32;
@@ -351,6 +365,7 @@ __device__ int gj_invert(double2* X, double2* Y, double2* Z, int n, const Lane& 
                          double2** out) {
   static_assert(NP <= 64, "pivot keys carry a 6-bit row index");
   constexpr int NTH = Geo<NP>::NTH;
+  const bool tw = (int)(threadIdx.x >> 5) < Geo<NP>::NW;  // this warp owns a tile
   constexpr int PE = NP * 8;                  // panel elements
   constexpr int PPT = (PE + NTH - 1) / NTH;   // panel elements per thread
   const int tid = threadIdx.x, lane = tid & 31;
@@ -513,7 +528,7 @@ __device__ int gj_invert(double2* X, double2* Y, double2* Z, int n, const Lane& 
         const int r = own_r(L, q), cc = own_c(L, j2, q);
         double2 v = c.get(j2, q);
         if (cc >= k0 && cc < k0 + 8) v = cmul(P[pidx(srow[q >> 1], cc - k0)], il);
-        nxt[sidx<NP>(r, cc)] = v;
+        if (tw) nxt[sidx<NP>(r, cc)] = v;
       }
     for (int j = 0; j < jmax; ++j) {
       const int k = k0 + j, b2 = sh.pivlog[k];
@@ -531,7 +546,7 @@ __device__ int gj_invert(double2* X, double2* Y, double2* Z, int n, const Lane& 
 #pragma unroll
   for (int e = 0; e < 8; ++e) {
     const int ri = (e & 3) >> 1, ci = (e >> 2) * 2 + (e & 1);
-    nxt[rbase[ri] + (cols[ci] ^ rsw[ri])] = cur[rbase[ri] + (scol[ci] ^ rsw[ri])];
+    if (tw) nxt[rbase[ri] + (cols[ci] ^ rsw[ri])] = cur[rbase[ri] + (scol[ci] ^ rsw[ri])];
   }
   __syncthreads();
   *out = nxt;
@@ -758,6 +773,7 @@ __global__ void __launch_bounds__(Geo<NP>::NTH, 1) sr_f64_kernel(SrArgs a) {
     for (int j = 0; j < 2; ++j)
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
+        if (!((sp.jt >> j) & 1)) continue;
         const int r = own_r(L, q), c = own_c(L, j, q);
         const double2 es = pes[sidx<NP>(r, c)];
         double2 v;
@@ -852,16 +868,16 @@ __global__ void __launch_bounds__(Geo<NP>::NTH, 1) rgf_f64_kernel(RgfArgs a) {
       load_mat<NP>(pc, V, n, nl);
       load_mat<NP>(bW, g, nl, nl);
       __syncthreads();
-      cmm<NP, false, false>(c1, pc, bW, lch, Ln);
-      store_acc<NP>(bU, c1, Ln);
+      cmm<NP, false, false>(c1, pc, bW, lch, Ln, sp.jt);
+      store_acc<NP>(bU, c1, Ln, sp.jt);
       __syncthreads();
-      cmm<NP, false, true>(c1, bU, pc, lch, Ln);
+      cmm<NP, false, true>(c1, bU, pc, lch, Ln, sp.jt);
 #pragma unroll
       for (int j = 0; j < 2; ++j)
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
           const int r = own_r(Ln, q), c = own_c(Ln, j, q);
-          if (r < n && c < n) S[r * n + c] = c1.get(j, q);
+          if (((sp.jt >> j) & 1) && r < n && c < n) S[r * n + c] = c1.get(j, q);
         }
       __syncthreads();
     }
@@ -871,6 +887,7 @@ __global__ void __launch_bounds__(Geo<NP>::NTH, 1) rgf_f64_kernel(RgfArgs a) {
     for (int j = 0; j < 2; ++j)
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
+        if (!((sp.jt >> j) & 1)) continue;
         const int r = own_r(Ln, q), c = own_c(Ln, j, q);
         double2 v;
         if (r < n && c < n) {
@@ -892,6 +909,7 @@ __global__ void __launch_bounds__(Geo<NP>::NTH, 1) rgf_f64_kernel(RgfArgs a) {
       for (int j = 0; j < 2; ++j)
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
+          if (!((sp.jt >> j) & 1)) continue;
           const int e = sidx<NP>(own_r(Ln, q), own_c(Ln, j, q));
           bG0[e] = pg[e];
         }
@@ -954,6 +972,7 @@ __global__ void __launch_bounds__(Geo<NP>::NTH, 1) rgf_f64_kernel(RgfArgs a) {
       for (int j = 0; j < 2; ++j)
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
+          if (!((sp.jt >> j) & 1)) continue;
           const int r = own_r(Ln, q), c = own_c(Ln, j, q);
           double2 gl = make_double2(0.0, 0.0), gr = gl;
           if (r < n && c < n) {
@@ -966,15 +985,16 @@ __global__ void __launch_bounds__(Geo<NP>::NTH, 1) rgf_f64_kernel(RgfArgs a) {
           bW[sidx<NP>(r, c)] = gr;
         }
       __syncthreads();
-      cmm<NP, false, false>(c1, pc, bG0, kch, Ln);
-      store_acc<NP>(bU, c1, Ln);
+      cmm<NP, false, false>(c1, pc, bG0, kch, Ln, sp.jt);
+      store_acc<NP>(bU, c1, Ln, sp.jt);
       __syncthreads();
-      cmm<NP, false, false>(c1, bU, bW, kch, Ln);
+      cmm<NP, false, false>(c1, bU, bW, kch, Ln, sp.jt);
       double t = 0.0;
 #pragma unroll
       for (int j = 0; j < 2; ++j)
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
+          if (!((sp.jt >> j) & 1)) continue;
           const double2 g = bG0[sidx<NP>(own_r(Ln, q), own_c(Ln, j, q))];
           t += c1.re[j][q] * g.x + c1.im[j][q] * g.y;
         }
