@@ -307,17 +307,21 @@ struct GJShared {
   int* sig;       // logical -> physical row within the current panel
   int* siginv;    // physical -> logical
   int* pivlog;    // pivlog[k]: logical row interchanged with row k at step k
+  int* cmap;      // cmap[c] = t_k(...t_0(c)) over the steps done so far
+  int* cmapinv;   // its inverse
   unsigned* key;  // [8] pivot key of each panel column
 };
 template <int NP>
-__host__ __device__ constexpr int gj_shared_bytes() { return 3 * NP * 4 + 8 * 4; }
+__host__ __device__ constexpr int gj_shared_bytes() { return 5 * NP * 4 + 8 * 4; }
 template <int NP>
 __device__ __forceinline__ GJShared carve_gj(unsigned char* base) {
   GJShared g;
   g.sig = reinterpret_cast<int*>(base);
   g.siginv = g.sig + NP;
   g.pivlog = g.siginv + NP;
-  g.key = reinterpret_cast<unsigned*>(g.pivlog + NP);
+  g.cmap = g.pivlog + NP;
+  g.cmapinv = g.cmap + NP;
+  g.key = reinterpret_cast<unsigned*>(g.cmapinv + NP);
   return g;
 }
 // Panel element (row r, column c < 8), rows of 8 with the row swizzle.
@@ -378,9 +382,13 @@ __device__ int gj_invert(double2* X, double2* Y, double2* Z, int n, const Lane& 
     rbase[ri] = rows[ri] * NP;
     rsw[ri] = swz(rows[ri]);
   }
-  int cols[4], scol[4];
+  int cols[4];
 #pragma unroll
-  for (int ci = 0; ci < 4; ++ci) cols[ci] = scol[ci] = L.n0 + 8 * (ci >> 1) + 2 * L.t + (ci & 1);
+  for (int ci = 0; ci < 4; ++ci) cols[ci] = L.n0 + 8 * (ci >> 1) + 2 * L.t + (ci & 1);
+  for (int c = tid; c < NP; c += NTH) {  // visible after the first panel's barrier
+    sh.cmap[c] = c;
+    sh.cmapinv[c] = c;
+  }
   // Panel elements owned by this thread: element e = tid + q NTH.  A partly
   // filled last slot (n = 48: 96 elements) goes to warps 1, 2, 3 rather
   // than 0, 1, 2, so that each of the SM's four sub-partitions (warp index
@@ -479,7 +487,8 @@ __device__ int gj_invert(double2* X, double2* Y, double2* Z, int n, const Lane& 
       P = Pn;
       Pn = t;
     }
-    // ---- rank-8 update of the whole matrix (all warps) ----
+    // ---- rank-8 update of the whole matrix (tile warps) ----
+    if (tw) {
     const double2 il = crecip_smith(lam);
     CAcc c;
     int srow[2];
@@ -528,14 +537,22 @@ __device__ int gj_invert(double2* X, double2* Y, double2* Z, int n, const Lane& 
         const int r = own_r(L, q), cc = own_c(L, j2, q);
         double2 v = c.get(j2, q);
         if (cc >= k0 && cc < k0 + 8) v = cmul(P[pidx(srow[q >> 1], cc - k0)], il);
-        if (tw) nxt[sidx<NP>(r, cc)] = v;
+        nxt[sidx<NP>(r, cc)] = v;
       }
-    for (int j = 0; j < jmax; ++j) {
-      const int k = k0 + j, b2 = sh.pivlog[k];
-#pragma unroll
-      for (int ci = 0; ci < 4; ++ci) {
-        const int scc = scol[ci];
-        scol[ci] = (scc == k) ? b2 : ((scc == b2) ? k : scc);
+    }
+    // The panel's interchanges t_k = (k pivlog_k) applied to the column map,
+    // by the bookkeeping thread (at n = 48 a warp without rank-8 work):
+    // cmap <- t_k o cmap swaps the two entries holding the values k and b.
+    if (tid == NTH - 32) {
+      for (int j = 0; j < jmax; ++j) {
+        const int k = k0 + j, b2 = sh.pivlog[k];
+        if (b2 != k) {
+          const int c1 = sh.cmapinv[k], c2 = sh.cmapinv[b2];
+          sh.cmap[c1] = b2;
+          sh.cmap[c2] = k;
+          sh.cmapinv[k] = c2;
+          sh.cmapinv[b2] = c1;
+        }
       }
     }
     __syncthreads();
@@ -546,7 +563,7 @@ __device__ int gj_invert(double2* X, double2* Y, double2* Z, int n, const Lane& 
 #pragma unroll
   for (int e = 0; e < 8; ++e) {
     const int ri = (e & 3) >> 1, ci = (e >> 2) * 2 + (e & 1);
-    if (tw) nxt[rbase[ri] + (cols[ci] ^ rsw[ri])] = cur[rbase[ri] + (scol[ci] ^ rsw[ri])];
+    if (tw) nxt[rbase[ri] + (cols[ci] ^ rsw[ri])] = cur[rbase[ri] + (sh.cmap[cols[ci]] ^ rsw[ri])];
   }
   __syncthreads();
   *out = nxt;
