@@ -210,6 +210,32 @@ __device__ __forceinline__ void cmm2b(CAcc& c1, CAcc& c2, const double2* A1, con
   }
 }
 
+// c1 = A B1, c2 = A B2 (the A fragments loaded once; each accumulator sees
+// the same tensor instructions as a separate cmm).
+template <int NP>
+__device__ __forceinline__ void cmm2a(CAcc& c1, CAcc& c2, const double2* A, const double2* B1, const double2* B2,
+                                      int kch, const Lane& L, int jm = 3) {
+  int ab[4], bb[2][2];
+  a_bases<NP, false>(L, ab);
+  b_bases<NP, false>(L, bb);
+  c1.zero();
+  c2.zero();
+  if (!jm) return;
+  for (int kc = 0; kc < kch; ++kc) {
+    double ar[4], ai[4];
+    load_a<NP, false>(A, ab, kc * 8, ar, ai);
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      if (!((jm >> j) & 1)) continue;
+      double br[2], bi[2];
+      load_b<NP, false>(B1, bb[j], kc * 8, br, bi);
+      cmma(c1.re[j], c1.im[j], ar, ai, br, bi);
+      load_b<NP, false>(B2, bb[j], kc * 8, br, bi);
+      cmma(c2.re[j], c2.im[j], ar, ai, br, bi);
+    }
+  }
+}
+
 template <int NP>
 __device__ __forceinline__ void store_acc(double2* S, const CAcc& c, const Lane& L, int jm = 3) {
 #pragma unroll
@@ -688,9 +714,13 @@ __global__ void __launch_bounds__(Geo<NP>::NTH, 1) sr_f64_kernel(SrArgs a) {
       store_acc<NP>(pbg, c2, sp.Lx, 2);
     }
     __syncthreads();
-    // eps_s += (alpha g) beta ; eps += (alpha g) beta + (beta g) alpha
+    // Pass A, shared A = alpha g: eps_s += (alpha g) beta, eps += (alpha g) beta,
+    // alpha' = (alpha g) alpha into the free g buffer.
+    // Pass B, shared A = beta g: eps += (beta g) alpha, beta' = (beta g) beta
+    // (stored after the barrier that ends every read of alpha and beta).
     int bad = 0;
-    cmm<NP, false, false>(c1, pag, pb, kch, L, sp.jm);
+    double e2 = 0.0;
+    cmm2a<NP>(c1, c2, pag, pb, pa, kch, L, sp.jm);
 #pragma unroll
     for (int j = 0; j < 2; ++j)
 #pragma unroll
@@ -701,9 +731,12 @@ __global__ void __launch_bounds__(Geo<NP>::NTH, 1) sr_f64_kernel(SrArgs a) {
         pes[e] = es;
         eps[j * 4 + q] = cadd(eps[j * 4 + q], c1.get(j, q));
         bad |= !cfinite(es);
+        bad |= !cfinite(c2.get(j, q));
+        e2 = fmax(e2, cabs2(c2.get(j, q)));
       }
+    store_acc<NP>(pg, c2, L, sp.jm);
     if (sp.extra) {
-      cmm<NP, false, false>(c1, pag, pb, kch, sp.Lx, 2);
+      cmm2a<NP>(c1, c2, pag, pb, pa, kch, sp.Lx, 2);
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
         const int e = sidx<NP>(own_r(sp.Lx, q), own_c(sp.Lx, 1, q));
@@ -711,9 +744,12 @@ __global__ void __launch_bounds__(Geo<NP>::NTH, 1) sr_f64_kernel(SrArgs a) {
         pes[e] = es;
         epsx[q * 32 + lane] = cadd(epsx[q * 32 + lane], c1.get(1, q));
         bad |= !cfinite(es);
+        bad |= !cfinite(c2.get(1, q));
+        e2 = fmax(e2, cabs2(c2.get(1, q)));
       }
+      store_acc<NP>(pg, c2, sp.Lx, 2);
     }
-    cmm<NP, false, false>(c1, pbg, pa, kch, L, sp.jm);
+    cmm2a<NP>(c1, c2, pbg, pa, pb, kch, L, sp.jm);
 #pragma unroll
     for (int j = 0; j < 2; ++j)
 #pragma unroll
@@ -721,56 +757,22 @@ __global__ void __launch_bounds__(Geo<NP>::NTH, 1) sr_f64_kernel(SrArgs a) {
         if (!((sp.jm >> j) & 1)) continue;
         eps[j * 4 + q] = cadd(eps[j * 4 + q], c1.get(j, q));
         bad |= !cfinite(eps[j * 4 + q]);
+        bad |= !cfinite(c2.get(j, q));
+        e2 = fmax(e2, cabs2(c2.get(j, q)));
       }
-    if (sp.extra) {
-      cmm<NP, false, false>(c1, pbg, pa, kch, sp.Lx, 2);
+    if (sp.extra) {  // the helper owns no tile, so c2 is free for the moved half's beta'
+      cmm2a<NP>(c1, c2, pbg, pa, pb, kch, sp.Lx, 2);
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
         const double2 e = cadd(epsx[q * 32 + lane], c1.get(1, q));
         epsx[q * 32 + lane] = e;
         bad |= !cfinite(e);
-      }
-    }
-    // alpha' = (alpha g) alpha into the free g buffer ; beta' = (beta g) beta
-    double e2 = 0.0;
-    cmm<NP, false, false>(c1, pag, pa, kch, L, sp.jm);
-#pragma unroll
-    for (int j = 0; j < 2; ++j)
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        if (!((sp.jm >> j) & 1)) continue;
-        bad |= !cfinite(c1.get(j, q));
-        e2 = fmax(e2, cabs2(c1.get(j, q)));
-      }
-    store_acc<NP>(pg, c1, L, sp.jm);
-    if (sp.extra) {
-      cmm<NP, false, false>(c1, pag, pa, kch, sp.Lx, 2);
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        bad |= !cfinite(c1.get(1, q));
-        e2 = fmax(e2, cabs2(c1.get(1, q)));
-      }
-      store_acc<NP>(pg, c1, sp.Lx, 2);
-    }
-    cmm<NP, false, false>(c1, pbg, pb, kch, L, sp.jm);
-#pragma unroll
-    for (int j = 0; j < 2; ++j)
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        if (!((sp.jm >> j) & 1)) continue;
-        bad |= !cfinite(c1.get(j, q));
-        e2 = fmax(e2, cabs2(c1.get(j, q)));
-      }
-    if (sp.extra) {  // beta' of the moved half waits in c2 for the barrier
-      cmm<NP, false, false>(c2, pbg, pb, kch, sp.Lx, 2);
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
         bad |= !cfinite(c2.get(1, q));
         e2 = fmax(e2, cabs2(c2.get(1, q)));
       }
     }
     __syncthreads();  // every read of alpha and beta is done
-    store_acc<NP>(pb, c1, L, sp.jm);
+    store_acc<NP>(pb, c2, L, sp.jm);
     if (sp.extra) store_acc<NP>(pb, c2, sp.Lx, 2);
     f0 = pa;  // old alpha buffer is free
     f1 = pag;
