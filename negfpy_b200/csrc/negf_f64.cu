@@ -840,8 +840,9 @@ __global__ void __launch_bounds__(Geo<NP>::NTH, 1) rgf_f64_kernel(RgfArgs a) {
   double2* const bW = b1 + MAT;
   double2* const bU = bW + MAT;
   double2* const bG0 = bU + MAT;
-  const GJShared gsh = carve_gj<NP>(reinterpret_cast<unsigned char*>(bG0 + MAT));
-  double* red = carve_red<NP>(bG0 + MAT);
+  double2* const bC = bG0 + MAT;  // the coupling block C of the current layer
+  const GJShared gsh = carve_gj<NP>(reinterpret_cast<unsigned char*>(bC + MAT));
+  double* red = carve_red<NP>(bC + MAT);
   __shared__ int s_point;
 
   const int n = a.n, L = a.L;
@@ -933,14 +934,17 @@ __global__ void __launch_bounds__(Geo<NP>::NTH, 1) rgf_f64_kernel(RgfArgs a) {
           bG0[e] = pg[e];
         }
       for (int l = 1; l < L && status == kOk; ++l) {
-        load_mat<NP>(pc, C + (long long)(l - 1) * a.c_ls, n, n);
-        __syncthreads();
+        // identical layers (layer stride 0) share one C: load it once per point
+        if (l == 1 || a.c_ls != 0) {
+          load_mat<NP>(bC, C + (long long)(l - 1) * a.c_ls, n, n);
+          __syncthreads();
+        }
         // W = g_{l-1} C, U = G_{0,l-1} C
-        cmm2b<NP>(c1, c2, pg, bG0, pc, kch, Ln, sp.jm);
+        cmm2b<NP>(c1, c2, pg, bG0, bC, kch, Ln, sp.jm);
         store_acc<NP>(bW, c1, Ln, sp.jm);
         store_acc<NP>(bU, c2, Ln, sp.jm);
         if (sp.extra) {
-          cmm2b<NP>(c1, c2, pg, bG0, pc, kch, sp.Lx, 2);
+          cmm2b<NP>(c1, c2, pg, bG0, bC, kch, sp.Lx, 2);
           store_acc<NP>(bW, c1, sp.Lx, 2);
           store_acc<NP>(bU, c2, sp.Lx, 2);
         }
@@ -949,7 +953,7 @@ __global__ void __launch_bounds__(Geo<NP>::NTH, 1) rgf_f64_kernel(RgfArgs a) {
         const double2* Dl = D + (long long)l * a.d_ls;
         const bool last = (l == L - 1);
         auto form_m = [&](const Lane& Lm, int jm) {
-          cmm<NP, true, false>(c1, pc, bW, kch, Lm, jm);
+          cmm<NP, true, false>(c1, bC, bW, kch, Lm, jm);
 #pragma unroll
           for (int j = 0; j < 2; ++j)
 #pragma unroll
@@ -969,7 +973,7 @@ __global__ void __launch_bounds__(Geo<NP>::NTH, 1) rgf_f64_kernel(RgfArgs a) {
         };
         form_m(Ln, sp.jm);
         if (sp.extra) form_m(sp.Lx, 2);
-        __syncthreads();  // C is dead once M is formed: pc becomes the second inversion buffer
+        __syncthreads();
         status = gj_invert<NP>(pg, pc, bW, n, Ln, gsh, &inv);
         if (status != kOk) break;
         pc = (inv == pg) ? pc : pg;
@@ -1262,7 +1266,7 @@ __global__ void heat_current_kernel(const double* __restrict__ om, const double*
 
 // ---------------------------------------------------------------- launchers --
 template <int NP>
-static size_t smem_bytes() { return (size_t)5 * Geo<NP>::MAT * 16 + tail_bytes<NP>(); }
+static size_t smem_bytes() { return (size_t)6 * Geo<NP>::MAT * 16 + tail_bytes<NP>(); }
 template <int NP>
 static size_t sr_smem_bytes() {
   return (size_t)6 * Geo<NP>::MAT * 16 + tail_bytes<NP>() + (Split<NP>::on ? 4 * 32 * 16 : 0);  // + epsx
