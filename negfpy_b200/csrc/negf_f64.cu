@@ -465,8 +465,9 @@ __device__ int gj_invert(double2* X, double2* Y, double2* Z, int n, const Lane& 
       const int pr = 63 - (int)(key & 63u);
       const int ex = (int)(key >> 20);
       const double sc = (ex != 0 && ex < 2046) ? __hiloint2double((2046 - ex) << 20, 0) : 1.0;
-      // Row interchange bookkeeping by the last warp: at n = 48 it owns one
-      // panel slot where warps 0-2 own two, so it waits least on the barrier.
+      // Row interchange bookkeeping by the last warp: at n = 48 a warp with
+      // no product tile, which also keeps the column map during the rank-8
+      // update.
       if (tid == NTH - 32) {
         const int k = k0 + j;
         const int bl = sh.siginv[pr];
