@@ -246,11 +246,12 @@ __device__ __forceinline__ void store_acc(double2* S, const CAcc& c, const Lane&
 }
 
 // Work split of the products between the SM's four sub-partitions (warp
-// index mod 4).  With 9 warps (NP = 48) sub-partition 0 runs warps 0, 4
-// and 8; the right half (j = 1) of warp 8's tile is done by warp 3
-// instead, so the sub-partitions carry 5, 4, 4 and 5 halves, not 6, 4, 4, 4.
-// The moved half keeps its arithmetic; its eps lives in shared memory
-// (lane-private, epsx[q * 32 + lane]) and is owned by warp 3.
+// index mod 4).  With 9 tiles (NP = 48) sub-partition 0 runs the tile
+// warps 0, 4 and 8; the right half (j = 1) of tile 8 is computed by a warp
+// of sub-partition 3 (kHelper) instead, so the sub-partitions carry 5, 4, 4
+// and 5 halves, not 6, 4, 4, 4.  The moved half keeps its arithmetic; in
+// the decimation its eps lives in shared memory (lane-private,
+// epsx[q * 32 + lane]), owned by the helper.
 template <int NP>
 struct Split {
   static constexpr bool on = Geo<NP>::NW == 9;
@@ -264,11 +265,11 @@ struct Split {
   __device__ __forceinline__ explicit Split(const Lane& L) {
     const int w = threadIdx.x >> 5;
     jt = w < Geo<NP>::NW ? 3 : 0;
-    jm = (on && w == 8) ? 1 : jt;
+    jm = (on && w == Geo<NP>::NW - 1) ? 1 : jt;
     extra = on && w == kHelper;
-    Lx = L;
-    Lx.m0 = 32;
-    Lx.n0 = 32;
+    Lx = L;  // the last tile (NW - 1) of the T x T grid
+    Lx.m0 = ((Geo<NP>::NW - 1) / Geo<NP>::T) * 16;
+    Lx.n0 = ((Geo<NP>::NW - 1) % Geo<NP>::T) * 16;
   }
 };
 
