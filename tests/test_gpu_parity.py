@@ -184,7 +184,7 @@ def test_slab_full_grid_properties_and_oracle_sample():
     assert rel_err(got, ref).max() <= TOL_T
 
 
-@pytest.mark.parametrize("n", [3, 16, 29, 48])
+@pytest.mark.parametrize("n", [3, 16, 29, 40, 47, 48])
 @pytest.mark.parametrize("scale", [1e-200, 1e-3, 1.0, 1e5, 1e200])
 def test_inversion_against_numpy(n, scale):
     """With d01 = 0 the decimation ends after one sweep with g = (z - d00)^-1,
@@ -230,6 +230,28 @@ def test_inversion_large_orders_against_numpy(n):
     g = nb.surface_gf(0.7, d00, np.zeros((n, n)), eta=0.01)
     err = np.max(np.abs(g - ref)) / np.max(np.abs(ref))
     assert err <= 1e-12 * np.linalg.cond(m), err
+
+
+def test_padded_order_48_transmission_vs_oracle():
+    """n = 42 (14 atoms x 3 DOF) runs on the n = 48 kernels with 6 padding
+    rows and columns: T against the oracle at four (omega, k) points."""
+    from negfpy_b200.models import material_kspace_device, material_kspace_lead
+
+    p = W.spring_network(6, ny=2, nz=7, periodic_y=True, periodic_z=False)
+    assert p.ndof == 42
+    wmax = W.estimate_omega_max(p, nk=6)
+    eta = 1e-5 * wmax * wmax
+    kp = [(0.9,), (-2.4,)]
+    lead, dev = material_kspace_lead(p), material_kspace_device(7, p)
+    om = np.array([0.31, 0.67]) * wmax
+    r = nb.transmission_grid(om, kp, dev, lead, lead, eta=eta)
+    assert np.all(r["status"] == 0)
+    for wi in range(2):
+        for ki in range(2):
+            d = dev.device(kp[ki])
+            lb = lead.blocks(kp[ki])
+            ref = O.transmission_point(float(om[wi]), list(d.onsite_blocks), list(d.coupling_blocks), lb, lb, eta=eta)
+            assert abs(r["T"][wi, ki] - ref) <= TOL_T * max(1.0, abs(ref)), (wi, ki, r["T"][wi, ki], ref)
 
 
 def test_largest_block_order_transmission_vs_oracle():
