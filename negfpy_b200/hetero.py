@@ -174,7 +174,12 @@ class HeteroModel:
     def blocks(self, theta: torch.Tensor, kpoints, masses: torch.Tensor | None = None, device=None):
         """(onsite [K, L, n, n], coupling [K, L-1, n, n]) complex128 for spring
         values theta and device site masses ``masses`` ``[L, ny*nz]`` (default
-        the model's); differentiable in both with torch autograd."""
+        the model's); differentiable in both with torch autograd.
+
+        The spring contributions are summed with ``index_add``, which on a CUDA
+        device adds in run-dependent order: the blocks, and T through them,
+        vary at rounding level between runs unless
+        ``torch.use_deterministic_algorithms(True)`` is set."""
         dev = device or theta.device
         ky = torch.as_tensor(np.array([k[0] for k in kpoints], float), device=dev)
         K, L, n = ky.numel(), self.L, self.n
