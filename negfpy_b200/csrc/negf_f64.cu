@@ -294,39 +294,6 @@ __device__ __forceinline__ double2 crecip_smith(double2 v) {
   return make_double2(r * i, -i);
 }
 
-// 2^(1023 - e) for the larger component exponent e of v: scales v so that
-// max(|re|, |im|) lies in [1, 2).  1 for zero/subnormal or huge components.
-__device__ __forceinline__ double pow2_normalizer(double2 v) {
-  const int ha = __double2hiint(v.x) & 0x7fffffff, hb = __double2hiint(v.y) & 0x7fffffff;
-  const int e = (ha > hb ? ha : hb) >> 20;
-  return (e != 0 && e < 2046) ? __hiloint2double((2046 - e) << 20, 0) : 1.0;
-}
-
-// 1 / p for a nonzero, finite complex p without FP64 division: p is scaled
-// by a power of two sc (exact) so that max(|re|, |im|) of p sc lies in
-// [1, 2); 1/|p sc|^2 comes from an fp32 reciprocal seed refined by two
-// Newton-Raphson steps y <- y + y (1 - d y) in FP64 (quadratic convergence:
-// 2^-22 -> 2^-44 -> below FP64 rounding); 1/p = sc conj(p sc) y.  Values
-// whose larger component is subnormal or near overflow use Smith's
-// algorithm instead.
-__device__ __forceinline__ float rcp_approx_f32(float x) {
-  float y;
-  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
-  return y;
-}
-__device__ __forceinline__ double2 crecip_fast(double2 v) {
-  const int ha = __double2hiint(v.x) & 0x7fffffff, hb = __double2hiint(v.y) & 0x7fffffff;
-  const int e = (ha > hb ? ha : hb) >> 20;
-  if (e == 0 || e >= 2046) return crecip_smith(v);
-  const double sc = __hiloint2double((2046 - e) << 20, 0);  // 2^(1023 - e)
-  const double as = v.x * sc, bs = v.y * sc;
-  const double d = fma(as, as, bs * bs);  // in [1, 8)
-  double y = (double)rcp_approx_f32((float)d);
-  y = fma(y, fma(-d, y, 1.0), y);
-  y = fma(y, fma(-d, y, 1.0), y);
-  return make_double2((as * y) * sc, -(bs * y) * sc);
-}
-
 // ---------------------------------------------------------- Gauss-Jordan --
 // Shared bookkeeping of the blocked Gauss-Jordan inversion (the panel itself
 // lives in a caller-provided free matrix buffer).
