@@ -44,7 +44,6 @@ __device__ __forceinline__ double2 crecip(double2 v) {
     return make_double2(r / d, -1.0 / d);
   }
 }
-__device__ __forceinline__ double cabs1(double2 a) { return fabs(a.x) + fabs(a.y); }
 __device__ __forceinline__ double cabs2(double2 a) { return a.x * a.x + a.y * a.y; }
 __device__ __forceinline__ bool cfinite(double2 a) { return isfinite(a.x) && isfinite(a.y); }
 

@@ -115,14 +115,6 @@ __device__ __forceinline__ void a_bases(const Lane& L, int (&base)[4]) {
     base[q] = CT ? sidx<NP>(kk, r) : sidx<NP>(r, kk);
   }
 }
-// A fragment bases into a row-stride-8 panel (16 x 8 at rows m0..).
-__device__ __forceinline__ void a_bases8(const Lane& L, int (&base)[4]) {
-#pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    const int r = L.m0 + L.g + 8 * (q & 1), kk = L.t + 4 * (q >> 1);
-    base[q] = r * 8 + (kk ^ swz(r));
-  }
-}
 template <int NP, bool CT>
 __device__ __forceinline__ void b_bases(const Lane& L, int (&base)[2][2]) {
 #pragma unroll

@@ -17,7 +17,6 @@ using glob::tc;
 using glob::tile_of;
 using glob::tr;
 
-__device__ __forceinline__ float2 fadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ float2 fneg(float2 a) { return make_float2(-a.x, -a.y); }
 __device__ __forceinline__ float2 fmulc(float2 a, float2 b) {
   return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
