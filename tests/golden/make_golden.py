@@ -244,10 +244,65 @@ def interface(out_dir: Path) -> None:
     np.savez_compressed(out_dir / "interface.npz", **out)
 
 
+DOS_KPOINTS = [(0.0, 0.0), (1.1, -0.6), (-2.5, 2.2), (2.9, 0.4)]
+
+
+def poisoned_blocks(lead, k):
+    """The lead's blocks, with NaN everywhere at the last k point of DOS_KPOINTS."""
+    d00, d01, d10 = (np.array(b, dtype=complex) for b in lead.blocks(k))
+    if tuple(k) == DOS_KPOINTS[-1]:
+        d00 = np.full_like(d00, np.nan)
+    return d00, d01, d10
+
+
+def dos(out_dir: Path) -> None:
+    """dos.npz: negfpy's k-averaged, adaptive and spectrum forms of the lead
+    surface DOS (core/dos.py:64-252) on a 2D-k material lead (n = 12) and on
+    the two different leads of its interface contacts."""
+    import json
+
+    import negfpy.core.dos as D
+    from negfpy.models.material_kspace import MaterialKspaceParams, material_kspace_lead
+    from negfpy.workflows import ifc_bulk
+
+    from negfpy_b200 import workloads as W
+
+    from negfpy.core.types import LeadKSpace
+
+    prm = interface_params("bulk", MaterialKspaceParams)
+    lead = material_kspace_lead(prm)
+    ll, lr, _, _ = ifc_bulk._build_interface_contacts(prm)
+    wmax = W.estimate_omega_max(prm, nk=6, two_d=True)
+    eta = 1e-5 * wmax * wmax
+    om = np.array([0.17, 0.45, 0.83]) * wmax
+    # The ladder's failure path, made deterministic: the last k point has NaN
+    # blocks, so it fails at every eta and counts as failed.
+    ladder = (1e-5 * wmax * wmax, 1e-3 * wmax * wmax)
+    poisoned = LeadKSpace(blocks_builder=lambda k: poisoned_blocks(lead, k))
+    out = {"omegas": om, "eta": eta, "ladder": np.array(ladder)}
+    out["kavg"] = np.array([D.lead_surface_dos_kavg(float(w), lead, DOS_KPOINTS, eta) for w in om])
+    out["kavg_norm"] = np.array([D.lead_surface_dos_kavg(float(w), lead, DOS_KPOINTS, eta, normalize_per_mode=True)
+                                 for w in om])
+    vals, infos = [], []
+    for w in om:
+        v, info = D.lead_surface_dos_kavg_adaptive(float(w), poisoned, DOS_KPOINTS, ladder, 0.5)
+        vals.append(v)
+        infos.append(info)
+    out["adaptive"] = np.array(vals)
+    out["adaptive_info"] = np.array(json.dumps(infos))
+    out["spectrum_k"] = D.lead_surface_dos_spectrum(om, lead, kpoints=DOS_KPOINTS, eta=eta)
+    out["spectrum_ladder"] = D.lead_surface_dos_spectrum(om, poisoned, kpoints=DOS_KPOINTS, eta_values=ladder,
+                                                         min_success_fraction=0.5)
+    out["spectrum_gamma"] = D.lead_surface_dos_spectrum(om, lead, eta=eta)
+    two = D.leads_surface_dos_spectrum(om, ll, lr, kpoints=DOS_KPOINTS, eta=eta, normalize_per_mode=True)
+    out["leads_left"], out["leads_right"] = two["left"], two["right"]
+    np.savez_compressed(out_dir / "dos.npz", **out)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference/src")
-    ap.add_argument("--only", choices=["thermal", "green", "workflow", "interface"], default=None,
+    ap.add_argument("--only", choices=["thermal", "green", "workflow", "interface", "dos"], default=None,
                     help="write one fixture file only")
     args = ap.parse_args()
     sys.path.insert(0, args.ref)
@@ -266,6 +321,10 @@ def main() -> None:
     if args.only == "interface":
         interface(OUT)
         print("wrote interface.npz")
+        return
+    if args.only == "dos":
+        dos(OUT)
+        print("wrote dos.npz")
         return
     import negfpy.core as R
     from negfpy.core.types import Device1D, LeadBlocks
