@@ -17,6 +17,7 @@ few points also with the QEP eigen method as an independent cross-check.
 from __future__ import annotations
 
 import argparse
+import os
 import sys
 from pathlib import Path
 
@@ -299,10 +300,106 @@ def dos(out_dir: Path) -> None:
     np.savez_compressed(out_dir / "dos.npz", **out)
 
 
+# negfpy's own study runs of real materials: (fixture name, run directory
+# under negfpy's studies/).  Each run directory holds the configuration the
+# run used (input.json), the transmission it wrote (transmission.tsv) and its
+# eta records (transmission_eta_diag.json).
+STUDY_RUNS = [
+    ("silicon_x", "silicon_bulk_2026q1/silicon/runs/20260225_033931Z_silicon_transmission_x"),
+    ("tan_x", "TaN/TaN/runs/20260225_113114Z_tan_transmission_x"),
+    ("graphene", "graphene_bulk_2026q1/graphene/runs/20260226_033848Z_graphene_transmission"),
+    ("phosphorene_x", "phosphorene_p_zerostrain_2026q1/phosphorene_p_zerostrain/runs/"
+                      "20260226_032511Z_phosphorene_p_zerostrain_transmission_x_area"),
+    ("borophene_y", "borophene_b_2x1_pbe_2026q1/borophene_b_2x1_pbe/runs/"
+                    "20260225_033229Z_borophene_b_2x1_pbe_transmission_y"),
+]
+
+
+def study_setup(run_dir: Path):
+    """The inputs negfpy's run_ifc_bulk hands to _run_transmission for one
+    study run (workflows/ifc_bulk.py:2186-2296): IFC read, reoriented and
+    cut, the material parameters with their mass mode and transverse
+    controls, the device layer count, the k meshes and the omega grid."""
+    import json
+
+    from negfpy.workflows import ifc_bulk as IB
+
+    cfg = json.loads((run_dir / "input.json").read_text())
+    cfg_dir = run_dir.parents[2] / "inputs" / "configs"
+    icfg, mcfg = dict(cfg.get("ifc", {})), dict(cfg.get("model", {}))
+    ifc = IB.read_ifc(IB._resolve_path(cfg_dir, icfg.get("path", "si444.fc")), reader=str(icfg.get("reader", "qe")))
+    if bool(icfg.get("enforce_asr", False)):
+        ifc, _ = IB.enforce_translational_asr_on_self_term(ifc)
+    ifc = IB._reorient_ifc_for_transport_direction(ifc, direction=int(mcfg.get("transport_direction", 1)))
+    cut = lambda key: None if icfg.get(key) is None else int(icfg[key])  # noqa: E731
+    ifc, _ = IB._apply_transverse_cutoff(ifc, dy_cutoff=cut("dy_cutoff"), dz_cutoff=cut("dz_cutoff"))
+    pls = mcfg.get("principal_layer_size", None)
+    bc = IB.BuildConfig(onsite_pinning=float(mcfg.get("onsite_pinning", 0.0)),
+                        principal_layer_size=None if pls is None else int(pls),
+                        auto_principal_layer_enlargement=bool(mcfg.get("auto_principal_layer_enlargement", True)),
+                        infer_fc01_from_negative_dx=bool(mcfg.get("infer_fc01_from_negative_dx", True)),
+                        enforce_hermitian_fc00=bool(mcfg.get("enforce_hermitian_fc00", True)),
+                        nyquist_split_half=bool(mcfg.get("nyquist_split_half", False)),
+                        dtype=str(mcfg.get("dtype", "complex128")))
+    prm = IB.build_material_kspace_params(ifc=ifc, config=bc)
+    prm, _ = IB._apply_mass_mode(prm, mcfg.get("mass_mode", "ifc"))
+    prm, _, _ = IB._apply_transverse_stability_controls(prm, ifc_metadata=dict(ifc.metadata),
+                                                        drop_nyquist=bool(mcfg.get("drop_nyquist_transverse", False)))
+    omegas, _ = IB._build_omega_grid(cfg, ifc)
+    return cfg, prm, int(mcfg.get("n_layers", 30)), IB._prepare_kmesh(cfg), omegas
+
+
+def _real_if_real(a):
+    a = np.asarray(a)
+    return a.real.copy() if np.iscomplexobj(a) and not np.any(a.imag) else a
+
+
+def studies(out_dir: Path, studies_root: Path) -> None:
+    """studies.npz: the material parameters, meshes and grids of negfpy's study
+    runs (study_setup), with the transmission and eta records those runs
+    wrote (negfpy's output files, computed with the QEP surface GF), and the
+    same workflow stage re-run here by negfpy with Sancho-Rubio (``sr_*``)."""
+    import json
+
+    from negfpy.workflows import ifc_bulk as IB
+
+    out = {}
+    for name, rel in STUDY_RUNS:
+        run = studies_root / rel
+        cfg, prm, n_layers, kmesh, omegas = study_setup(run)
+        ll, lr, vdl_l, vdl_r = IB._build_interface_contacts(prm)
+        dev = IB.material_kspace_device(n_layers=n_layers, params=prm)
+        sr_cfg = json.loads(json.dumps(cfg))
+        sr_cfg["solver"]["surface_gf_method"] = "sancho_rubio"
+        sr_cfg["solver"]["parallel"] = {"enabled": True, "backend": "process", "workers": os.cpu_count() or 1}
+        res = IB._run_transmission(sr_cfg, device=dev, lead_left=ll, lead_right=lr, device_to_lead_left=vdl_l,
+                                   device_to_lead_right=vdl_r, omegas=omegas, kmesh=kmesh)
+        out[f"{name}_sr_values"] = np.asarray(res["values"], dtype=float)
+        meta = {k: res[k] for k in ("eta_records", "omega_failures", "n_rejected_total")}
+        out[f"{name}_sr_meta"] = np.array(json.dumps(meta, default=lambda o: list(o) if isinstance(o, tuple) else o))
+        tsv = np.loadtxt(run / "transmission.tsv")
+        assert np.abs(tsv[:, 0] - omegas).max() <= 1e-12 * max(1.0, float(np.abs(omegas).max())), name
+        diag = json.loads((run / "transmission_eta_diag.json").read_text())
+        out[f"{name}_cfg"] = np.array(json.dumps(cfg))
+        out[f"{name}_kmesh"] = np.array(json.dumps(kmesh, default=list))
+        out[f"{name}_omegas"] = np.asarray(omegas, dtype=float)
+        out[f"{name}_n_layers"] = n_layers
+        out[f"{name}_T"] = tsv[:, 3].copy()
+        out[f"{name}_diag"] = np.array(json.dumps(diag))
+        out[f"{name}_masses"] = np.asarray(prm.masses, dtype=float)
+        out[f"{name}_pinning"] = float(prm.onsite_pinning)
+        out[f"{name}_dof"] = int(prm.dof_per_atom)
+        for key in ("fc00", "fc01", "fc10"):
+            terms = getattr(prm, key + "_terms")
+            if terms is not None:
+                out.update(_terms_arrays(f"{name}_{key}", {k: _real_if_real(v) for k, v in terms.items()}))
+    np.savez_compressed(out_dir / "studies.npz", **out)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference/src")
-    ap.add_argument("--only", choices=["thermal", "green", "workflow", "interface", "dos"], default=None,
+    ap.add_argument("--only", choices=["thermal", "green", "workflow", "interface", "dos", "studies"], default=None,
                     help="write one fixture file only")
     args = ap.parse_args()
     sys.path.insert(0, args.ref)
@@ -325,6 +422,11 @@ def main() -> None:
     if args.only == "dos":
         dos(OUT)
         print("wrote dos.npz")
+        return
+    studies_root = Path(args.ref).resolve().parent / "studies"
+    if args.only == "studies":
+        studies(OUT, studies_root)
+        print("wrote studies.npz")
         return
     import negfpy.core as R
     from negfpy.core.types import Device1D, LeadBlocks
@@ -441,6 +543,9 @@ def main() -> None:
     thermal(OUT)
     green(OUT)
     workflow(OUT)
+    interface(OUT)
+    dos(OUT)
+    studies(OUT, studies_root)
     print("wrote", sorted(p.name for p in OUT.glob("*.npz")))
 
 

@@ -1,0 +1,69 @@
+"""negfpy's own study runs of real materials (silicon, TaN, graphene,
+phosphorene, borophene; n = 12 to 72, 2 to 40 layers, 1D and 2D k meshes)
+through the workflow's transmission stage on the GPU, from the material
+parameters to the k-averaged T(omega) and its eta records
+(tests/golden/studies.npz).
+
+The reference values are negfpy's _run_transmission on the same inputs with
+the Sancho-Rubio surface GF (tests/test_studies_fixture.py ties them to the
+transmission.tsv files those runs wrote with the QEP surface GF).  Bound:
+1e-10 max(|T|, 1) per omega, and equal eta records.
+"""
+
+from __future__ import annotations
+
+import json
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+from negfpy_b200 import workflow as WF  # noqa: E402
+from negfpy_b200.models import MaterialKspaceParams, interface_contacts, material_kspace_device  # noqa: E402
+from tests.conftest import GOLDEN  # noqa: E402
+from tests.golden.make_golden import STUDY_RUNS  # noqa: E402
+from tests.test_gpu_workflow import _close, _norm  # noqa: E402
+
+TOL = 1e-10
+
+
+@pytest.fixture(scope="module")
+def fix():
+    return np.load(GOLDEN / "studies.npz")
+
+
+def study_params(fix, name: str) -> MaterialKspaceParams:
+    def terms(key):
+        if f"{name}_{key}_keys" not in fix.files:
+            return None
+        return {tuple(int(x) for x in k): b for k, b in zip(fix[f"{name}_{key}_keys"], fix[f"{name}_{key}_blocks"])}
+
+    return MaterialKspaceParams(masses=fix[f"{name}_masses"], fc00_terms=terms("fc00"), fc01_terms=terms("fc01"),
+                                fc10_terms=terms("fc10"), dof_per_atom=int(fix[f"{name}_dof"]),
+                                onsite_pinning=float(fix[f"{name}_pinning"]))
+
+
+def study_kmesh(fix, name: str) -> dict:
+    km = json.loads(str(fix[f"{name}_kmesh"]))
+    for part in ("low", "high"):
+        km[part]["kpoints"] = [tuple(k) for k in km[part]["kpoints"]]
+    return km
+
+
+@pytest.mark.parametrize("name", [n for n, _ in STUDY_RUNS])
+def test_study_run_matches_negfpy(fix, name):
+    cfg = json.loads(str(fix[f"{name}_cfg"]))
+    cfg["solver"]["surface_gf_method"] = "sancho_rubio"
+    prm = study_params(fix, name)
+    ll, lr, vdl_l, vdl_r = interface_contacts(prm)
+    dev = material_kspace_device(n_layers=int(fix[f"{name}_n_layers"]), params=prm)
+    res = WF.run_transmission(cfg, device=dev, lead_left=ll, lead_right=lr, device_to_lead_left=vdl_l,
+                              device_to_lead_right=vdl_r, omegas=fix[f"{name}_omegas"], kmesh=study_kmesh(fix, name))
+    v, ref = np.asarray(res["values"]), fix[f"{name}_sr_values"]
+    assert np.array_equal(np.isnan(v), np.isnan(ref))
+    ok = ~np.isnan(ref)
+    err = np.abs(v[ok] - ref[ok]) / np.maximum(np.abs(ref[ok]), 1.0)
+    assert err.max(initial=0.0) <= TOL, (name, int(np.argmax(err)), float(err.max()))
+    meta = json.loads(str(fix[f"{name}_sr_meta"]))
+    _close(_norm({k: res[k] for k in ("eta_records", "omega_failures", "n_rejected_total")}), meta, 1e-12)
