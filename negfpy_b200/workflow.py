@@ -339,3 +339,191 @@ def run_transmission(cfg: dict[str, Any], *, device, lead_left, lead_right, devi
             "n_omega_failures": len(omega_failures),
         },
     }
+
+
+def compute_fcs_k_moments(cfg: dict[str, Any], *, device, lead_left, lead_right, device_to_lead_left=None,
+                          device_to_lead_right=None, omegas: np.ndarray, kmesh: dict[str, Any]) -> dict[str, Any]:
+    """<T>_k and <T^2>_k per omega with one eta per omega (negfpy
+    ``workflows/ifc_bulk.py:1690-1784``, ``_compute_fcs_k_moments``).
+
+    The first eta of the omega's ladder (or ``eta_fixed``) at which at least
+    one k point and at least ``min_success_fraction`` of them give a finite T
+    no lower than ``-nonnegative_tolerance`` is taken; the moments are the
+    means of max(T, 0) and its square over those k points.  Each rung is ONE
+    launch per k mesh over every omega still without an accepted eta."""
+    scfg = dict(cfg.get("solver", {}))
+    sgf_method = str(scfg.get("surface_gf_method", "generalized_eigen_svd"))
+    eta_fixed = float(scfg.get("eta_fixed", 1e-4))
+    eta_values_base = tuple(float(v) for v in scfg.get("eta_values", DEFAULT_ETA_VALUES))
+    eta_device_raw = scfg.get("eta_device", None)
+    eta_device = None if eta_device_raw is None else float(eta_device_raw)
+    min_success_fraction = float(scfg.get("min_success_fraction", 0.7))
+    nonnegative_tolerance = float(scfg.get("nonnegative_tolerance", 1e-8))
+    max_eta_over_omega_raw = scfg.get("max_eta_over_omega", None)
+    max_eta_over_omega = None if max_eta_over_omega_raw is None else float(max_eta_over_omega_raw)
+    eta_ratio_cm1_min_raw = scfg.get("eta_ratio_cm1_min", None)
+    eta_ratio_cm1_min = None if eta_ratio_cm1_min_raw is None else float(eta_ratio_cm1_min_raw)
+    eta_scheme = str(scfg.get("eta_scheme", "adaptive_global")).lower().replace("-", "_")
+    if eta_scheme not in {"fixed", "adaptive_global"}:
+        eta_scheme = "adaptive_global"
+    check_method(sgf_method)
+
+    omegas = np.asarray(omegas, dtype=float)
+    W = int(omegas.size)
+    t_mean = np.full((W,), np.nan, dtype=float)
+    t2_mean = np.full((W,), np.nan, dtype=float)
+    eta_selected = np.full((W,), np.nan, dtype=float)
+    n_k_success = np.zeros((W,), dtype=int)
+    meshes: dict[str, _Mesh] = {}
+    tasks = {}  # omega index -> [omega, omega_cm1, mesh name, etas to try]
+    for i, w in enumerate(omegas):
+        w = float(w)
+        if w <= 0.0:
+            t_mean[i] = 0.0
+            t2_mean[i] = 0.0
+            continue
+        w_cm1 = float(np.asarray(qe_omega_to_cm1(w), dtype=float))
+        name = "low" if w_cm1 <= float(kmesh["low_cm1"]) else "high"
+        ladder = resolve_eta_values_for_omega(w, w_cm1, eta_values=eta_values_base,
+                                              max_eta_over_omega=max_eta_over_omega,
+                                              eta_ratio_cm1_min=eta_ratio_cm1_min)
+        eta_try = (eta_fixed,) if eta_scheme == "fixed" else ladder
+        if len(kmesh[name]["kpoints"]) > 0 and name not in meshes:
+            meshes[name] = _Mesh(kmesh[name]["kpoints"], device, lead_left, lead_right, eta_device,
+                                 device_to_lead_left, device_to_lead_right, None, None)
+        tasks[i] = [w, w_cm1, name, tuple(float(e) for e in eta_try)]
+
+    pending = [i for i in tasks if tasks[i][2] in meshes]
+    rung = 0
+    while pending:
+        batch: dict[str, list] = {}
+        for i in pending:
+            w, _, name, etas = tasks[i]
+            if rung < len(etas):
+                batch.setdefault(name, []).extend((i, k) for k in range(len(meshes[name].kpoints)))
+        if not batch:
+            break
+        done = set()
+        for name, pts in batch.items():
+            mesh = meshes[name]
+            K = len(mesh.kpoints)
+            T, st = _solve(mesh, [tasks[i][0] for i, _ in pts], [tasks[i][3][rung] for i, _ in pts],
+                           [k for _, k in pts])
+            for j in range(0, len(pts), K):
+                i = pts[j][0]
+                vals = np.array([max(float(t), 0.0) for t, s in zip(T[j:j + K], st[j:j + K])
+                                 if _classify(t, s, None, nonnegative_tolerance) is None], dtype=float)
+                frac = float(vals.size / max(K, 1))
+                if vals.size > 0 and frac >= min_success_fraction:
+                    t_mean[i] = float(np.mean(vals))
+                    t2_mean[i] = float(np.mean(vals * vals))
+                    eta_selected[i] = tasks[i][3][rung]
+                    n_k_success[i] = int(vals.size)
+                    done.add(i)
+        pending = [i for i in pending if i not in done]
+        rung += 1
+    omega_failures = [{"omega_qe": tasks[i][0], "omega_cm1": tasks[i][1], "reason": "no_eta_passed_threshold"}
+                      for i in sorted(tasks) if not np.isfinite(t_mean[i])]
+    return {"t_mean": t_mean, "t2_mean": t2_mean, "eta_selected": eta_selected, "n_k_success": n_k_success,
+            "omega_failures": omega_failures}
+
+
+def run_fcs(cfg: dict[str, Any], *, omegas: np.ndarray, kmesh: dict[str, Any], device, lead_left, lead_right,
+            device_to_lead_left=None, device_to_lead_right=None, area_m2: float | None) -> dict[str, Any]:
+    """The workflow's full-counting-statistics stage (negfpy
+    ``workflows/ifc_bulk.py:1787-1935``, ``_run_fcs``): the k moments
+    (``compute_fcs_k_moments``), then C1, C2 and the finite-time uncertainty
+    over the temperature sweep, with the spectral integrals on the GPU.  Same
+    configuration keys, checks, messages and result dictionary."""
+    from .fcs import heat_current_cumulants_from_k_moments, heat_current_uncertainty
+
+    fcfg = dict(cfg.get("fcs", {}))
+    x_mode = str(fcfg.get("x", "temperature")).lower().replace("-", "_")
+    y_mode = str(fcfg.get("y", "conductance_per_area")).lower().replace("-", "_")
+    if x_mode not in {"temperature", "temperature_bias"}:
+        raise ValueError("fcs.x must be 'temperature' or 'temperature_bias'.")
+    if y_mode not in {"heat_current", "heat_current_per_area", "conductance", "conductance_per_area"}:
+        raise ValueError("fcs.y must be one of: heat_current, heat_current_per_area, conductance, conductance_per_area.")
+    t_min = float(fcfg.get("temperature_min_k", 50.0))
+    t_max = float(fcfg.get("temperature_max_k", 1000.0))
+    n_points = int(fcfg.get("n_points", 120))
+    tau_s = float(fcfg.get("measurement_time_s", 1e-6))
+    if n_points < 2:
+        raise ValueError("fcs.n_points must be >= 2.")
+    if tau_s <= 0.0:
+        raise ValueError("fcs.measurement_time_s must be positive.")
+
+    moments = compute_fcs_k_moments(cfg, device=device, lead_left=lead_left, lead_right=lead_right,
+                                    device_to_lead_left=device_to_lead_left, device_to_lead_right=device_to_lead_right,
+                                    omegas=omegas, kmesh=kmesh)
+    omega_rad_s = np.asarray(qe_omega_to_rad_s(omegas), dtype=float)
+    valid = np.isfinite(moments["t_mean"]) & np.isfinite(moments["t2_mean"])
+    if int(np.sum(valid)) < 2:
+        raise RuntimeError("FCS failed: insufficient converged omega points.")
+    om = omega_rad_s[valid]
+    t1 = np.asarray(moments["t_mean"], dtype=float)[valid]
+    t2 = np.asarray(moments["t2_mean"], dtype=float)[valid]
+
+    xvals = np.linspace(t_min, t_max, n_points, endpoint=True)
+    if x_mode == "temperature":
+        temp_mode = str(fcfg.get("temperature_mode", "fixed_delta")).lower().replace("-", "_")
+        if temp_mode == "fixed_right":
+            t_left = xvals
+            t_right = np.full_like(xvals, float(fcfg.get("temperature_right_k", 300.0)))
+            x_label = "Temperature Left (K)"
+        else:
+            dT = float(fcfg.get("delta_t_k", 10.0))
+            if dT <= 0.0:
+                raise ValueError("fcs.delta_t_k must be positive.")
+            t_left = xvals + 0.5 * dT
+            t_right = xvals - 0.5 * dT
+            x_label = "Average Temperature (K)"
+    else:
+        tavg = float(fcfg.get("temperature_avg_k", 300.0))
+        t_left = tavg + 0.5 * xvals
+        t_right = tavg - 0.5 * xvals
+        x_label = "Temperature Bias (K)"
+    if np.any(t_left <= 0.0) or np.any(t_right <= 0.0):
+        raise ValueError("FCS sweep generates non-positive temperatures.")
+
+    y = np.zeros_like(xvals, dtype=float)
+    y_std = np.zeros_like(xvals, dtype=float)
+    c1 = np.zeros_like(xvals, dtype=float)
+    c2 = np.zeros_like(xvals, dtype=float)
+    for i in range(xvals.size):
+        cc = heat_current_cumulants_from_k_moments(om, t1, t2, float(t_left[i]), float(t_right[i]))
+        uu = heat_current_uncertainty(cc, measurement_time_s=tau_s)
+        c1[i] = float(cc.c1_j_per_s)
+        c2[i] = float(cc.c2_j2_per_s)
+        if y_mode in {"conductance", "conductance_per_area"}:
+            dtemp = float(t_left[i] - t_right[i])
+            if abs(dtemp) < 1e-12:
+                y[i] = np.nan
+                y_std[i] = np.nan
+            else:
+                y[i] = float(c1[i] / dtemp)
+                y_std[i] = float(uu.std_current_j_per_s / abs(dtemp))
+        else:
+            y[i] = float(c1[i])
+            y_std[i] = float(uu.std_current_j_per_s)
+    if y_mode in {"heat_current_per_area", "conductance_per_area"}:
+        if area_m2 is None or area_m2 <= 0.0:
+            raise ValueError("FCS y-mode requests per-area quantity but area is unavailable.")
+        y = y / float(area_m2)
+        y_std = y_std / float(area_m2)
+    y_label = {"heat_current": "Heat Current (J/s)", "heat_current_per_area": "Heat Current per Area (J/s/m^2)",
+               "conductance": "Thermal Conductance (W/K)"}.get(y_mode, "Thermal Conductance per Area (W/m^2/K)")
+    n_conv = int(np.sum(valid))
+    return {
+        "x_mode": x_mode, "x_label": x_label, "y_mode": y_mode, "y_label": y_label, "x": xvals,
+        "temp_left_k": t_left, "temp_right_k": t_right, "y": y, "y_std": y_std, "c1_j_per_s": c1,
+        "c2_j2_per_s": c2, "measurement_time_s": float(tau_s), "omega_qe": np.asarray(omegas, dtype=float),
+        "omega_rad_s_valid": om, "t_mean_valid": t1, "t2_mean_valid": t2,
+        "t_mean": np.asarray(moments["t_mean"], dtype=float), "t2_mean": np.asarray(moments["t2_mean"], dtype=float),
+        "eta_selected": np.asarray(moments["eta_selected"], dtype=float),
+        "n_k_success": np.asarray(moments["n_k_success"], dtype=int),
+        "omega_failures": list(moments["omega_failures"]), "n_omega_converged": n_conv,
+        "n_omega_total": int(len(omegas)),
+        "summary": {"x_mode": x_mode, "y_mode": y_mode, "measurement_time_s": float(tau_s),
+                    "n_omega_converged": n_conv, "n_omega_total": int(len(omegas))},
+    }

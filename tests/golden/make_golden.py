@@ -315,11 +315,13 @@ STUDY_RUNS = [
 ]
 
 
-def study_setup(run_dir: Path):
-    """The inputs negfpy's run_ifc_bulk hands to _run_transmission for one
-    study run (workflows/ifc_bulk.py:2186-2296): IFC read, reoriented and
-    cut, the material parameters with their mass mode and transverse
-    controls, the device layer count, the k meshes and the omega grid."""
+def study_setup(run_dir: Path, ifc_path: str | None = None):
+    """The inputs negfpy's run_ifc_bulk hands to _run_transmission (or
+    _run_fcs) for one study run (workflows/ifc_bulk.py:2186-2296): IFC read,
+    reoriented and cut, the material parameters with their mass mode and
+    transverse controls, the device layer count, the k meshes and the omega
+    grid.  ``ifc_path`` replaces a force-constant path that only existed on
+    the machine of the run, relative to the study's inputs/configs."""
     import json
 
     from negfpy.workflows import ifc_bulk as IB
@@ -327,6 +329,8 @@ def study_setup(run_dir: Path):
     cfg = json.loads((run_dir / "input.json").read_text())
     cfg_dir = run_dir.parents[2] / "inputs" / "configs"
     icfg, mcfg = dict(cfg.get("ifc", {})), dict(cfg.get("model", {}))
+    if ifc_path is not None:
+        icfg["path"] = ifc_path
     ifc = IB.read_ifc(IB._resolve_path(cfg_dir, icfg.get("path", "si444.fc")), reader=str(icfg.get("reader", "qe")))
     if bool(icfg.get("enforce_asr", False)):
         ifc, _ = IB.enforce_translational_asr_on_self_term(ifc)
@@ -346,7 +350,18 @@ def study_setup(run_dir: Path):
     prm, _, _ = IB._apply_transverse_stability_controls(prm, ifc_metadata=dict(ifc.metadata),
                                                         drop_nyquist=bool(mcfg.get("drop_nyquist_transverse", False)))
     omegas, _ = IB._build_omega_grid(cfg, ifc)
-    return cfg, prm, int(mcfg.get("n_layers", 30)), IB._prepare_kmesh(cfg), omegas
+    if ifc_path is None:
+        return cfg, prm, int(mcfg.get("n_layers", 30)), IB._prepare_kmesh(cfg), omegas
+    thick, tdir, lvo = (mcfg.get(k, None) for k in ("thickness_angstrom", "thickness_direction",
+                                                    "lattice_vectors_angstrom"))
+    lv = IB._resolve_lattice_vectors_for_area(
+        ifc_lattice_vectors=None if ifc.lattice_vectors is None else np.asarray(ifc.lattice_vectors, dtype=float),
+        ifc_metadata=dict(ifc.metadata),
+        lattice_vectors_override_angstrom=None if lvo is None else np.asarray(lvo, dtype=float))
+    area = IB._compute_effective_area_m2(lv, transport_direction=int(mcfg.get("transport_direction", 1)),
+                                         thickness_m=None if thick is None else float(thick) * IB.ANGSTROM_M,
+                                         thickness_direction=None if tdir is None else int(tdir))
+    return cfg, prm, int(mcfg.get("n_layers", 30)), IB._prepare_kmesh(cfg), omegas, float(area)
 
 
 def _real_if_real(a):
@@ -396,10 +411,95 @@ def studies(out_dir: Path, studies_root: Path) -> None:
     np.savez_compressed(out_dir / "studies.npz", **out)
 
 
+FCS_STUDY_RUN = "TaN/TaN/runs/20260304_104756Z_tan_x_fcs_cond_area_20260304"
+FCS_STUDY_IFC = "../../FORCE_CONSTANTS"  # the run's own path pointed at its author's machine
+# Configuration variants of the FCS stage on the silicon study's material, on
+# a 16/36-point k mesh: every x/y mode, the three temperature sweeps and the
+# fixed and global eta schemes.
+FCS_KMESH_CFG = {"dimension": 2, "mode": "shifted", "nk": 4, "nk_low": 6, "low_cm1": 120.0}
+FCS_CFGS = {
+    "delta_conductance": {
+        "solver": {"surface_gf_method": "sancho_rubio", "eta_scheme": "adaptive_global",
+                   "eta_values": [1e-8, 1e-6, 1e-4], "min_success_fraction": 0.7},
+        "fcs": {"x": "temperature", "y": "conductance", "temperature_mode": "fixed_delta", "delta_t_k": 5.0,
+                "temperature_min_k": 10.0, "temperature_max_k": 500.0, "n_points": 25}},
+    "right_heat_current": {
+        "solver": {"surface_gf_method": "sancho_rubio", "eta_scheme": "fixed", "eta_fixed": 1e-6},
+        "fcs": {"x": "temperature", "y": "heat_current", "temperature_mode": "fixed_right",
+                "temperature_right_k": 200.0, "temperature_min_k": 5.0, "temperature_max_k": 800.0, "n_points": 17,
+                "measurement_time_s": 3e-9}},
+    "bias_per_area": {
+        "solver": {"surface_gf_method": "sancho_rubio", "eta_scheme": "adaptive", "eta_values": [1e-8, 1e-7, 1e-5],
+                   "min_success_fraction": 1.0, "max_eta_over_omega": 2e-4, "eta_ratio_cm1_min": 50.0,
+                   "nonnegative_tolerance": 1e-12},
+        "fcs": {"x": "temperature_bias", "y": "heat_current_per_area", "temperature_avg_k": 300.0,
+                "temperature_min_k": -100.0, "temperature_max_k": 100.0, "n_points": 21}},
+}
+FCS_KEYS = ("t_mean", "t2_mean", "eta_selected", "n_k_success", "x", "temp_left_k", "temp_right_k", "y", "y_std",
+            "c1_j_per_s", "c2_j2_per_s")
+
+
+def fcs(out_dir: Path, studies_root: Path) -> None:
+    """fcs.npz: negfpy's FCS stage (_run_fcs, workflows/ifc_bulk.py:1690-1935)
+    with Sancho-Rubio on the silicon study's material for the FCS_CFGS
+    variants, and on the TaN FCS study run's inputs, whose own outputs
+    (fcs_moments.npz and fcs.tsv, written with the QEP surface GF) are stored
+    beside it as ``tan_pub_*``."""
+    import json
+
+    from negfpy.workflows import ifc_bulk as IB
+
+    out = {}
+
+    def run(prefix, cfg, prm, n_layers, kmesh, omegas, area):
+        ll, lr, vdl_l, vdl_r = IB._build_interface_contacts(prm)
+        dev = IB.material_kspace_device(n_layers=n_layers, params=prm)
+        res = IB._run_fcs(cfg, omegas=omegas, kmesh=kmesh, device=dev, lead_left=ll, lead_right=lr,
+                          device_to_lead_left=vdl_l, device_to_lead_right=vdl_r, area_m2=area)
+        for key in FCS_KEYS:
+            out[f"{prefix}_{key}"] = np.asarray(res[key])
+        out[f"{prefix}_failures"] = np.array(json.dumps(res["omega_failures"]))
+
+    def store_params(prefix, prm):
+        out[f"{prefix}_masses"] = np.asarray(prm.masses, dtype=float)
+        out[f"{prefix}_pinning"] = float(prm.onsite_pinning)
+        out[f"{prefix}_dof"] = int(prm.dof_per_atom)
+        for key in ("fc00", "fc01", "fc10"):
+            terms = getattr(prm, key + "_terms")
+            if terms is not None:
+                out.update(_terms_arrays(f"{prefix}_{key}", {k: _real_if_real(v) for k, v in terms.items()}))
+
+    si_run = studies_root / dict(STUDY_RUNS)["silicon_x"]
+    _, si_prm, si_layers, _, si_om = study_setup(si_run)
+    km = IB._prepare_kmesh({"kmesh": FCS_KMESH_CFG})
+    out["si_kmesh"] = np.array(json.dumps(km, default=list))
+    out["si_omegas"], out["si_n_layers"], out["si_area"] = si_om, si_layers, 3.1e-19
+    store_params("si", si_prm)
+    for name, cfg in FCS_CFGS.items():
+        run(name, cfg, si_prm, si_layers, km, si_om, 3.1e-19)
+
+    tan_run = studies_root / FCS_STUDY_RUN
+    cfg, prm, n_layers, kmesh, omegas, area = study_setup(tan_run, FCS_STUDY_IFC)
+    cfg["ifc"]["path"] = FCS_STUDY_IFC
+    out["tan_cfg"] = np.array(json.dumps(cfg))
+    out["tan_kmesh"] = np.array(json.dumps(kmesh, default=list))
+    out["tan_omegas"], out["tan_n_layers"], out["tan_area"] = omegas, n_layers, area
+    store_params("tan", prm)
+    pub = np.load(tan_run / "fcs_moments.npz")
+    assert np.abs(pub["omega_qe"] - omegas).max() <= 1e-12 * float(np.abs(omegas).max())
+    for key in ("t_mean", "t2_mean", "eta_selected", "n_k_success"):
+        out[f"tan_pub_{key}"] = pub[key]
+    out["tan_pub_table"] = np.loadtxt(tan_run / "fcs.tsv")
+    sr_cfg = json.loads(json.dumps(cfg))
+    sr_cfg["solver"]["surface_gf_method"] = "sancho_rubio"
+    run("tan_sr", sr_cfg, prm, n_layers, kmesh, omegas, area)
+    np.savez_compressed(out_dir / "fcs.npz", **out)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference/src")
-    ap.add_argument("--only", choices=["thermal", "green", "workflow", "interface", "dos", "studies"], default=None,
+    ap.add_argument("--only", choices=["thermal", "green", "workflow", "interface", "dos", "studies", "fcs"], default=None,
                     help="write one fixture file only")
     args = ap.parse_args()
     sys.path.insert(0, args.ref)
@@ -427,6 +527,10 @@ def main() -> None:
     if args.only == "studies":
         studies(OUT, studies_root)
         print("wrote studies.npz")
+        return
+    if args.only == "fcs":
+        fcs(OUT, studies_root)
+        print("wrote fcs.npz")
         return
     import negfpy.core as R
     from negfpy.core.types import Device1D, LeadBlocks
@@ -546,6 +650,7 @@ def main() -> None:
     interface(OUT)
     dos(OUT)
     studies(OUT, studies_root)
+    fcs(OUT, studies_root)
     print("wrote", sorted(p.name for p in OUT.glob("*.npz")))
 
 
