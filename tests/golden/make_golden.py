@@ -315,6 +315,27 @@ STUDY_RUNS = [
 ]
 
 
+# negfpy's thermal-conductance study runs: (fixture name, run directory).
+# Each turns the transmission.tsv of a transmission run into G(T) with the
+# workflow's _thermal_conductance_from_spectrum (workflows/ifc_bulk.py:408-438).
+THERMAL_RUNS = [
+    ("tan_x", "TaN/TaN/runs/20260225_120308Z_tan_thermal_x"),
+    ("silicon_x", "silicon_bulk_2026q1/silicon/runs/20260226_034402Z_silicon_thermal_x_area"),
+    ("graphene_x", "graphene_bulk_2026q1/graphene/runs/20260226_034402Z_graphene_thermal_x_area"),
+    ("borophene_y", "borophene_b_2x1_pbe_2026q1/borophene_b_2x1_pbe/runs/"
+                    "20260225_085015Z_borophene_b_2x1_pbe_thermal_y"),
+]
+
+
+def thermal_source(run_dir: Path) -> Path:
+    """The transmission.tsv a thermal run read (workflows/ifc_bulk.py:1444-1468)."""
+    import json
+
+    cfg = json.loads((run_dir / "input.json").read_text())
+    report = run_dir.parents[2] / "inputs" / "configs" / cfg["thermal"]["transmission_report_path"]
+    return report.resolve().parent / "transmission.tsv"
+
+
 def study_setup(run_dir: Path, ifc_path: str | None = None):
     """The inputs negfpy's run_ifc_bulk hands to _run_transmission (or
     _run_fcs) for one study run (workflows/ifc_bulk.py:2186-2296): IFC read,
@@ -408,6 +429,12 @@ def studies(out_dir: Path, studies_root: Path) -> None:
             terms = getattr(prm, key + "_terms")
             if terms is not None:
                 out.update(_terms_arrays(f"{name}_{key}", {k: _real_if_real(v) for k, v in terms.items()}))
+    for name, rel in THERMAL_RUNS:
+        run = studies_root / rel
+        src = np.loadtxt(thermal_source(run))
+        tab = np.loadtxt(run / "thermal_conductance.tsv")
+        out[f"thermal_{name}_spectrum"] = src  # omega_qe, THz, cm^-1, T[, T per m^2]
+        out[f"thermal_{name}_table"] = tab  # temperature, G, G per m^2
     np.savez_compressed(out_dir / "studies.npz", **out)
 
 

@@ -22,7 +22,7 @@ pytestmark = pytest.mark.gpu
 from negfpy_b200 import workflow as WF  # noqa: E402
 from negfpy_b200.models import MaterialKspaceParams, interface_contacts, material_kspace_device  # noqa: E402
 from tests.conftest import GOLDEN  # noqa: E402
-from tests.golden.make_golden import STUDY_RUNS  # noqa: E402
+from tests.golden.make_golden import STUDY_RUNS, THERMAL_RUNS  # noqa: E402
 from tests.test_gpu_workflow import _close, _norm  # noqa: E402
 
 TOL = 1e-10
@@ -67,3 +67,18 @@ def test_study_run_matches_negfpy(fix, name):
     assert err.max(initial=0.0) <= TOL, (name, int(np.argmax(err)), float(err.max()))
     meta = json.loads(str(fix[f"{name}_sr_meta"]))
     _close(_norm({k: res[k] for k in ("eta_records", "omega_failures", "n_rejected_total")}), meta, 1e-12)
+
+
+@pytest.mark.parametrize("name", [n for n, _ in THERMAL_RUNS])
+def test_thermal_study_conductance(fix, name):
+    """G(T) and G(T) per area of negfpy's thermal runs from the same spectra
+    (workflows/ifc_bulk.py:408-438, 1444-1505) with the kappa kernel."""
+    from negfpy_b200.spectrum import thermal_conductance_from_spectrum
+    from negfpy_b200.workflow import qe_omega_to_rad_s
+
+    spec, tab = fix[f"thermal_{name}_spectrum"], fix[f"thermal_{name}_table"]
+    unit = float(np.asarray(qe_omega_to_rad_s(1.0), dtype=float))
+    for col_t, col_g in ((3, 1), (4, 2)):
+        g = thermal_conductance_from_spectrum(spec[:, 0], spec[:, col_t], tab[:, 0], unit)
+        ref = tab[:, col_g]
+        assert np.abs(g - ref).max() <= 1e-11 * np.abs(ref).max(), (name, col_g)

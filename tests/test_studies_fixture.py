@@ -19,7 +19,7 @@ import numpy as np
 import pytest
 
 from tests.conftest import GOLDEN
-from tests.golden.make_golden import STUDY_RUNS
+from tests.golden.make_golden import STUDY_RUNS, THERMAL_RUNS
 
 LADDER_DIFFERS = {"tan_x": list(range(1, 30))}
 
@@ -98,3 +98,20 @@ def test_fcs_fixture_pinned_to_the_fcs_study_output():
     for key in ("t_mean", "t2_mean"):
         a, b = f[f"tan_pub_{key}"][same], f[f"tan_sr_{key}"][same]
         assert (np.abs(a - b) / np.maximum(np.abs(a), 1.0)).max() <= 5e-9, key
+
+
+@pytest.mark.parametrize("name", [n for n, _ in THERMAL_RUNS])
+def test_oracle_conductance_reproduces_the_thermal_study_output(fix, name):
+    """negfpy's thermal runs turned a transmission run's spectrum into G(T)
+    and G(T) per area (workflows/ifc_bulk.py:408-438, 1444-1505); the
+    oracle's restatement gives the same table from the same spectrum to the
+    table's printed precision (13 significant digits)."""
+    from negfpy_b200.workflow import qe_omega_to_rad_s
+    from oracle.negf_oracle import thermal_conductance
+
+    spec, tab = fix[f"thermal_{name}_spectrum"], fix[f"thermal_{name}_table"]
+    unit = float(np.asarray(qe_omega_to_rad_s(1.0), dtype=float))
+    for col_t, col_g in ((3, 1), (4, 2)):
+        g = thermal_conductance(spec[:, 0], spec[:, col_t], tab[:, 0], unit)
+        ref = tab[:, col_g]
+        assert np.abs(g - ref).max() <= 1e-11 * np.abs(ref).max(), (name, col_g)
