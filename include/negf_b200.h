@@ -13,7 +13,7 @@
  *    (NEGF_EINVAL bad argument, NEGF_EUNSUPPORTED size not built,
  *    NEGF_ECUDA CUDA error); negf_last_error() describes it.  Numerical
  *    outcomes are per point in `status_out`: NEGF_OK, NEGF_MAXITER,
- *    NEGF_NONFINITE, NEGF_SINGULAR, NEGF_REFINE_FAIL.
+ *    NEGF_NONFINITE, NEGF_SINGULAR, NEGF_REFINE_FAIL, NEGF_UNSTABLE.
  *
  * Each entry point names the negfpy routine it replaces (paths relative to
  * the negfpy project root).
@@ -35,6 +35,7 @@ extern "C" {
 #define NEGF_SINGULAR 3
 #define NEGF_REFINE_FAIL 4
 #define NEGF_BAD_ITEM 5 /* batch item: system, k index or block order out of range */
+#define NEGF_UNSTABLE 6 /* decimation: inf/nan arose inside an iteration from finite blocks */
 
 #define NEGF_EINVAL (-1)
 #define NEGF_EUNSUPPORTED (-2)

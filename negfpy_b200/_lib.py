@@ -17,9 +17,9 @@ from . import _build
 _lock = threading.Lock()
 _lib = None
 
-OK, MAXITER, NONFINITE, SINGULAR, REFINE_FAIL, BAD_ITEM = 0, 1, 2, 3, 4, 5
+OK, MAXITER, NONFINITE, SINGULAR, REFINE_FAIL, BAD_ITEM, UNSTABLE = 0, 1, 2, 3, 4, 5, 6
 STATUS_NAMES = {OK: "ok", MAXITER: "maxiter", NONFINITE: "non_finite", SINGULAR: "singular", REFINE_FAIL: "refine_failed",
-                BAD_ITEM: "bad_item"}
+                BAD_ITEM: "bad_item", UNSTABLE: "unstable"}
 
 _P = C.c_void_p
 _I = C.c_int

@@ -14,6 +14,7 @@ enum Status : int {
   kSingular = 3,    // exact zero pivot in an inversion
   kRefineFail = 4,  // mixed-precision refinement did not converge
   kBadItem = 5,     // batch item with an out-of-range system, k index or block order
+  kUnstable = 6,    // Sancho-Rubio: inf/nan arose inside an iteration from finite blocks
 };
 
 __device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
@@ -97,5 +98,25 @@ __device__ __forceinline__ double block_sum(double v, double* red) {
 }
 // Returns nonzero in every thread if any thread passed nonzero.
 __device__ __forceinline__ int block_any(int v) { return __syncthreads_or(v); }
+
+// The status of a decimation that met inf/nan in iteration `it` (an
+// inversion pivot, or the products and sums).  negfpy runs each iteration
+// under numpy's floating-point traps (core/surface_gf.py:40-56): an overflow
+// or invalid operation there is "numerically unstable", while inf/nan that
+// came in with the blocks pass through quietly and are "non-finite values".
+// Every iteration after the first starts from finite blocks, so only the
+// first can be the quiet case.  Every thread of the block calls this.
+__device__ __forceinline__ int sr_failure_status(int it, int n, const double2* h00, const double2* h01,
+                                                 const double2* h10, double2 z) {
+  int bad = 0;
+  if (it == 1) {
+    bad = !(isfinite(z.x) && isfinite(z.y));
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+      const double2 a = h00[e], b = h01[e], c = h10 ? h10[e] : make_double2(0.0, 0.0);
+      bad |= !(isfinite(a.x) && isfinite(a.y) && isfinite(b.x) && isfinite(b.y) && isfinite(c.x) && isfinite(c.y));
+    }
+  }
+  return block_any(bad) ? kNonFinite : kUnstable;
+}
 
 }  // namespace negf

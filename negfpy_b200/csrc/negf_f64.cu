@@ -743,6 +743,7 @@ __global__ void __launch_bounds__(Geo<NP>::NTH, 1) sr_f64_kernel(SrArgs a) {
     const double emax = block_max(e2, red);
     if (emax < tol2) { converged = true; break; }
   }
+  if (status == kNonFinite) status = sr_failure_status(it, n, h00, h01, h10, z);
   if (status == kOk && !converged) {
     status = kMaxIter;
     it = a.maxiter;
@@ -1019,7 +1020,12 @@ __global__ void sr_scalar_kernel(SrArgs a) {
     e = cadd(cadd(e, agb), bga);
     al = cmul(ag, al);
     be = cmul(bg, be);
-    if (!cfinite(es) || !cfinite(e) || !cfinite(al) || !cfinite(be)) { status = kNonFinite; break; }
+    if (!cfinite(es) || !cfinite(e) || !cfinite(al) || !cfinite(be)) {
+      // as sr_failure_status, for one thread's 1 x 1 blocks
+      const bool quiet = it == 1 && !(cfinite(h00) && cfinite(h01) && cfinite(h10) && cfinite(z));
+      status = quiet ? kNonFinite : kUnstable;
+      break;
+    }
     if (fmax(cabs2(al), cabs2(be)) < tol2) { conv = true; break; }
   }
   if (status == kOk && !conv) { status = kMaxIter; it = a.maxiter; }

@@ -24,6 +24,8 @@ QEP_NAMES = {
 MSG_NONFINITE = ("Sancho-Rubio decimation produced non-finite values. "
                  "Try a larger eta or a different surface_gf method.")
 MSG_MAXITER = "Sancho-Rubio decimation did not converge within maxiter."
+MSG_UNSTABLE = ("Sancho-Rubio decimation became numerically unstable. "
+                "Try a larger eta or a different surface_gf method.")
 
 
 def check_method(method: str) -> None:
@@ -48,6 +50,8 @@ def raise_for_status(status: int) -> None:
         raise RuntimeError(MSG_MAXITER)
     if status == _lib.NONFINITE:
         raise RuntimeError(MSG_NONFINITE)
+    if status == _lib.UNSTABLE:
+        raise RuntimeError(MSG_UNSTABLE)
     if status == _lib.SINGULAR:
         raise np.linalg.LinAlgError("Singular matrix")
     raise RuntimeError(f"NEGF kernel failed with status {status}")

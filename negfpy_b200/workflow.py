@@ -527,3 +527,212 @@ def run_fcs(cfg: dict[str, Any], *, omegas: np.ndarray, kmesh: dict[str, Any], d
         "summary": {"x_mode": x_mode, "y_mode": y_mode, "measurement_time_s": float(tau_s),
                     "n_omega_converged": n_conv, "n_omega_total": int(len(omegas))},
     }
+
+
+class _DosMesh:
+    """One k mesh of a lead, stacked once on the GPU for the DOS stage."""
+
+    def __init__(self, lead, kpoints):
+        from .dos import _stack_leads
+        from . import engine
+
+        self.kpoints = list(kpoints)
+        self.K = len(self.kpoints)
+        if self.K:
+            d00, d01, d10 = _stack_leads(lead, [k if len(k) > 0 else None for k in self.kpoints])
+            self.n = int(d00.shape[-1])
+            self.blocks = (engine._c(d00), engine._c(d01), None if d10 is None else engine._c(d10))
+
+    def solve(self, omegas: list, etas: list, ks: list, normalize_per_mode: bool):
+        """DOS and status of (omega, eta, k) points in one launch."""
+        from . import engine
+
+        dev = _lib.require_cuda()
+        if not omegas:
+            return np.zeros(0), np.zeros(0, dtype=np.int32)
+        r = engine.sgf_sr(*self.blocks, torch.tensor(omegas, dtype=torch.float64, device=dev),
+                          torch.tensor(etas, dtype=torch.float64, device=dev),
+                          torch.tensor(ks, dtype=torch.int32, device=dev), want_g=False, want_dos=True)
+        d = r["dos"].cpu().numpy()
+        return (d / self.n if normalize_per_mode else d), r["status"].cpu().numpy()
+
+
+def run_dos(cfg: dict[str, Any], *, lead, omegas: np.ndarray, kmesh: dict[str, Any]) -> dict[str, Any]:
+    """The workflow's surface-DOS stage (negfpy ``workflows/ifc_bulk.py:1290-1441``,
+    ``_run_dos``, with ``_lead_surface_dos_kavg_adaptive_global_eta``
+    ``:908-948``): per omega the k-mean DOS at ``eta_fixed``, with one eta per
+    omega (``adaptive_global``), or with negfpy's per-k ladder (any other
+    scheme), batched: each rung is ONE launch per k mesh over all pending
+    (omega, k) points.  Same configuration keys, acceptance rules, messages
+    and result dictionary."""
+    from .surface_gf import raise_for_status
+
+    scfg = dict(cfg.get("solver", {}))
+    dcfg = dict(cfg.get("dos", {}))
+    sgf_method = str(scfg.get("surface_gf_method", "generalized_eigen_svd"))
+    eta_scheme = str(scfg.get("eta_scheme", "adaptive")).lower().replace("-", "_")
+    eta_fixed = float(scfg.get("eta_fixed", 1e-4))
+    eta_values_base = tuple(float(v) for v in scfg.get("eta_values", DEFAULT_ETA_VALUES))
+    min_success_fraction = float(scfg.get("min_success_fraction", 0.7))
+    max_eta_over_omega_raw = scfg.get("max_eta_over_omega", None)
+    max_eta_over_omega = None if max_eta_over_omega_raw is None else float(max_eta_over_omega_raw)
+    eta_ratio_cm1_min_raw = scfg.get("eta_ratio_cm1_min", None)
+    eta_ratio_cm1_min = None if eta_ratio_cm1_min_raw is None else float(eta_ratio_cm1_min_raw)
+    normalize_per_mode = bool(dcfg.get("normalize_per_mode", False))
+    negative_tolerance = float(dcfg.get("negative_tolerance", 1e-12))
+    check_method(sgf_method)
+
+    omegas = np.asarray(omegas, dtype=float)
+    vals = np.zeros_like(omegas, dtype=float)
+    meshes: dict[str, _DosMesh] = {}
+    tasks: dict[int, dict] = {}
+    outcome: dict[int, tuple] = {}  # omega index -> (dos, info) or (None, error message)
+    for i, w in enumerate(omegas):
+        w = float(w)
+        if w < 0.0:
+            vals[i] = np.nan
+            continue
+        w_cm1 = float(np.asarray(qe_omega_to_cm1(w), dtype=float))
+        name = "low" if w_cm1 <= float(kmesh["low_cm1"]) else "high"
+        ladder = resolve_eta_values_for_omega(float(max(w, 1e-30)), w_cm1, eta_values=eta_values_base,
+                                              max_eta_over_omega=max_eta_over_omega,
+                                              eta_ratio_cm1_min=eta_ratio_cm1_min)
+        if name not in meshes:
+            meshes[name] = _DosMesh(lead, kmesh[name]["kpoints"])
+        K = meshes[name].K
+        t = {"w": w, "w_cm1": w_cm1, "name": name, "K": K}
+        if eta_scheme == "fixed":
+            if K == 0:
+                outcome[i] = (None, "kpoints must contain at least one k-point.")
+                continue
+            t["etas"], t["rule"] = (eta_fixed,), "fixed"
+        elif eta_scheme == "adaptive_global":
+            if K == 0 and ladder:
+                outcome[i] = (None, "division by zero")
+                continue
+            t["etas"], t["rule"] = ladder, "global"
+        else:
+            if K == 0:
+                outcome[i] = (None, "kpoints must contain at least one k-point.")
+                continue
+            if len(ladder) == 0:
+                outcome[i] = (None, "eta_values must contain at least one eta value.")
+                continue
+            if not (0.0 <= min_success_fraction <= 1.0):
+                outcome[i] = (None, "min_success_fraction must be in [0, 1].")
+                continue
+            t["etas"], t["rule"] = ladder, "per_k"
+            t["pending"], t["accepted"] = list(range(K)), {}
+        tasks[i] = t
+
+    pending = list(tasks)
+    rung = 0
+    while pending:
+        batch: dict[str, list] = {}
+        for i in pending:
+            t = tasks[i]
+            if rung < len(t["etas"]):
+                ks = t["pending"] if t["rule"] == "per_k" else range(t["K"])
+                batch.setdefault(t["name"], []).extend((i, k) for k in ks)
+        if not batch:
+            break
+        done = set()
+        for name, pts in batch.items():
+            d, st = meshes[name].solve([tasks[i]["w"] for i, _ in pts], [tasks[i]["etas"][rung] for i, _ in pts],
+                                       [k for _, k in pts], normalize_per_mode)
+            rows: dict[int, list] = {}
+            for (i, k), dv, sv in zip(pts, d, st):
+                rows.setdefault(i, []).append((k, float(dv), int(sv)))
+            for i, rr in rows.items():
+                t = tasks[i]
+                eta = t["etas"][rung]
+                if t["rule"] == "fixed":
+                    bad = [sv for _, _, sv in rr if sv != _lib.OK]
+                    if bad:
+                        try:
+                            raise_for_status(bad[0])
+                        except Exception as exc:  # negfpy's first failing k ends the k mean
+                            outcome[i] = (None, str(exc))
+                    else:
+                        K = t["K"]
+                        outcome[i] = (float(np.mean([dv for _, dv, _ in rr])),
+                                      {"n_total": K, "n_success": K, "n_failed": 0, "success_fraction": 1.0,
+                                       "eta_selected": float(eta_fixed), "eta_histogram": {float(eta_fixed): K}})
+                    done.add(i)
+                elif t["rule"] == "global":
+                    good = [float(max(dv, 0.0)) for _, dv, sv in rr
+                            if sv == _lib.OK and np.isfinite(dv) and not dv < -negative_tolerance]
+                    frac = float(len(good) / t["K"])
+                    if good and frac >= min_success_fraction:
+                        outcome[i] = (float(np.mean(good)),
+                                      {"n_total": t["K"], "n_success": len(good), "n_failed": t["K"] - len(good),
+                                       "success_fraction": frac, "eta_selected": float(eta),
+                                       "eta_histogram": {float(e): (len(good) if float(e) == float(eta) else 0)
+                                                         for e in t["etas"]}})
+                        done.add(i)
+                else:
+                    nxt = []
+                    for k, dv, sv in rr:
+                        if sv == _lib.OK and np.isfinite(dv):
+                            t["accepted"][k] = (dv, float(eta))
+                        else:
+                            nxt.append(k)
+                    t["pending"] = nxt
+                    if not nxt:
+                        done.add(i)
+        pending = [i for i in pending if i not in done]
+        rung += 1
+
+    for i, t in tasks.items():
+        if i in outcome:
+            continue
+        if t["rule"] == "global":
+            outcome[i] = (None, "No eta value satisfied global adaptive DOS quality threshold.")
+            continue
+        K, acc = t["K"], t["accepted"]
+        v = [acc[k][0] for k in range(K) if k in acc]
+        used = [acc[k][1] for k in range(K) if k in acc]
+        frac = float(len(v) / K)
+        if not v:
+            outcome[i] = (None, "No k-point converged for adaptive k-averaged DOS.")
+        elif frac < min_success_fraction:
+            outcome[i] = (None, "Adaptive k-averaged DOS failed success-fraction threshold "
+                                f"(got {frac:.3f}, required >= {min_success_fraction:.3f}).")
+        else:
+            outcome[i] = (float(np.mean(v)), {"n_total": K, "n_success": len(v), "n_failed": K - len(v),
+                                              "success_fraction": frac,
+                                              "eta_histogram": {float(e): int(sum(1 for u in used if u == float(e)))
+                                                                for e in t["etas"]}})
+
+    eta_records, omega_failures = [], []
+    for i in sorted(outcome):
+        w = float(omegas[i])
+        w_cm1 = float(np.asarray(qe_omega_to_cm1(w), dtype=float))
+        dval, info = outcome[i]
+        if dval is None:
+            vals[i] = np.nan
+            omega_failures.append({"omega_qe": w, "omega_cm1": w_cm1, "error": info})
+            continue
+        vals[i] = float(max(dval, 0.0))
+        hist = dict(info.get("eta_histogram", {}))
+        used_e = [float(e) for e, c in hist.items() if int(c) > 0]
+        max_eta_used = max(used_e) if used_e else np.nan
+        eta_records.append({
+            "omega_qe": w, "omega_cm1": w_cm1, "n_failed_kpoints": int(info.get("n_failed", 0)),
+            "success_fraction": float(info.get("success_fraction", 0.0)), "eta_histogram": hist,
+            "eta_selected": info.get("eta_selected", None),
+            "max_eta_used": None if not np.isfinite(max_eta_used) else float(max_eta_used),
+            "max_eta_over_omega": None if not np.isfinite(max_eta_used) or w <= 0.0 else float(max_eta_used / w),
+        })
+    if np.all(~np.isfinite(vals)):
+        raise RuntimeError("DOS calculation failed for all omega points.")
+    max_ratio = max((r["max_eta_over_omega"] for r in eta_records if r["max_eta_over_omega"] is not None),
+                    default=None)
+    return {
+        "values": vals,
+        "eta_records": eta_records,
+        "omega_failures": omega_failures,
+        "summary": {"surface_gf_method": sgf_method, "eta_scheme": eta_scheme, "eta_fixed": eta_fixed,
+                    "eta_values_base": eta_values_base, "normalize_per_mode": normalize_per_mode,
+                    "max_eta_over_omega": max_ratio, "n_omega_failures": len(omega_failures)},
+    }

@@ -523,10 +523,88 @@ def fcs(out_dir: Path, studies_root: Path) -> None:
     np.savez_compressed(out_dir / "fcs.npz", **out)
 
 
+# Configuration variants of the workflow's DOS stage on the right interface
+# lead of the silicon study's material (n = 12, the FCS k mesh), with a
+# negative omega; the "nan_*" variants poison one k point of the high mesh.
+# The study grid's omega = 0 is left out: there z = -eta^2 is real, and
+# whether the decimation converges or overflows at a k point depends on
+# rounding (as for eta = 0 at any omega).
+DOS_WORKFLOW_CFGS = {
+    "fixed": {"solver": {"surface_gf_method": "sancho_rubio", "eta_scheme": "fixed", "eta_fixed": 1e-6},
+              "dos": {"normalize_per_mode": True}},
+    "global": {"solver": {"surface_gf_method": "sancho_rubio", "eta_scheme": "adaptive_global",
+                          "eta_values": [1e-8, 1e-6, 1e-4], "min_success_fraction": 0.7, "max_eta_over_omega": 2e-3,
+                          "eta_ratio_cm1_min": 60.0}, "dos": {"negative_tolerance": 1e-10}},
+    "per_k": {"solver": {"surface_gf_method": "sancho_rubio", "eta_scheme": "adaptive", "eta_values": [1e-8, 1e-7],
+                         "min_success_fraction": 0.5}},
+    "nan_fixed": {"solver": {"surface_gf_method": "sancho_rubio", "eta_scheme": "fixed", "eta_fixed": 1e-6}},
+    "nan_global": {"solver": {"surface_gf_method": "sancho_rubio", "eta_scheme": "adaptive-global",
+                              "eta_values": [1e-8, 1e-6], "min_success_fraction": 0.9}},
+    "nan_per_k": {"solver": {"surface_gf_method": "sancho_rubio", "eta_scheme": "adaptive",
+                             "eta_values": [1e-8, 1e-6], "min_success_fraction": 0.95}},
+}
+DOS_NAN_K = 2  # index into the high k mesh
+
+
+def nan_at(lead, kbad):
+    """The lead's blocks, with NaN everywhere at k point ``kbad``."""
+    def blocks(k):
+        d00, d01, d10 = (np.array(b, dtype=complex) for b in lead.blocks(k))
+        if tuple(k) == tuple(kbad):
+            d00 = np.full_like(d00, np.nan)
+        return d00, d01, d10
+    return blocks
+
+
+def dos_workflow(out_dir: Path, studies_root: Path) -> None:
+    """dos_workflow.npz: negfpy's _run_dos (workflows/ifc_bulk.py:1290-1441)
+    with Sancho-Rubio for the DOS_WORKFLOW_CFGS variants."""
+    import json
+
+    from negfpy.core.types import LeadKSpace
+    from negfpy.workflows import ifc_bulk as IB
+
+    _, prm, _, _, om = study_setup(studies_root / dict(STUDY_RUNS)["silicon_x"])
+    km = IB._prepare_kmesh({"kmesh": FCS_KMESH_CFG})
+    omegas = np.concatenate([[-1e-4], om[1:]])
+    _, lead, _, _ = IB._build_interface_contacts(prm)
+    bad = LeadKSpace(blocks_builder=nan_at(lead, km["high"]["kpoints"][DOS_NAN_K]))
+    out = {"omegas": omegas, "kmesh": np.array(json.dumps(km, default=list))}
+    for name, cfg in DOS_WORKFLOW_CFGS.items():
+        res = IB._run_dos(cfg, lead=bad if name.startswith("nan") else lead, omegas=omegas, kmesh=km)
+        out[f"{name}_values"] = res["values"]
+        meta = {k: res[k] for k in ("eta_records", "omega_failures", "summary")}
+        out[f"{name}_meta"] = np.array(json.dumps(meta, default=lambda o: list(o) if isinstance(o, tuple) else o))
+    # negfpy's messages for a decimation that overflows from finite blocks and
+    # for NaN blocks, at the orders of the three kernel families
+    from negfpy.core import surface_gf
+
+    msgs = {}
+    for n in SR_FAILURE_ORDERS:
+        for case, (d00, d01) in sr_failure_blocks(n).items():
+            try:
+                surface_gf(0.5, d00, d01, eta=1e-8, method="sancho_rubio")
+                msgs[f"{case}_{n}"] = None
+            except Exception as exc:  # the message is the fixture
+                msgs[f"{case}_{n}"] = f"{type(exc).__name__}: {exc}"
+    out["sr_failure_messages"] = np.array(json.dumps(msgs))
+    np.savez_compressed(out_dir / "dos_workflow.npz", **out)
+
+
+SR_FAILURE_ORDERS = (1, 4, 64)
+
+
+def sr_failure_blocks(n: int) -> dict:
+    """Lead blocks whose decimation fails: coupling 1e200 (the first
+    iteration's products overflow from finite blocks) and NaN blocks."""
+    eye = np.eye(n, dtype=complex)
+    return {"overflow": (eye, 1e200 * eye), "nan": (np.full((n, n), np.nan, dtype=complex), eye)}
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference/src")
-    ap.add_argument("--only", choices=["thermal", "green", "workflow", "interface", "dos", "studies", "fcs"], default=None,
+    ap.add_argument("--only", choices=["thermal", "green", "workflow", "interface", "dos", "studies", "fcs", "dos_workflow"], default=None,
                     help="write one fixture file only")
     args = ap.parse_args()
     sys.path.insert(0, args.ref)
@@ -558,6 +636,10 @@ def main() -> None:
     if args.only == "fcs":
         fcs(OUT, studies_root)
         print("wrote fcs.npz")
+        return
+    if args.only == "dos_workflow":
+        dos_workflow(OUT, studies_root)
+        print("wrote dos_workflow.npz")
         return
     import negfpy.core as R
     from negfpy.core.types import Device1D, LeadBlocks
@@ -678,6 +760,7 @@ def main() -> None:
     dos(OUT)
     studies(OUT, studies_root)
     fcs(OUT, studies_root)
+    dos_workflow(OUT, studies_root)
     print("wrote", sorted(p.name for p in OUT.glob("*.npz")))
 
 

@@ -4,7 +4,7 @@ import numpy as np
 import pytest
 
 from oracle import negf_oracle as O
-from tests.conftest import rel_err
+from tests.conftest import GOLDEN, rel_err
 
 
 def test_chain_transmission_matches_reference(golden):
@@ -96,3 +96,19 @@ def test_bulk_n96_oracle_matches_reference():
         lead = (d00, d01, np.conj(d01).T)
         t = O.transmission_point(w, [d00] * L, [d01] * (L - 1), lead, lead, eta=float(g["eta"]))
         assert rel_err(t, g["T"][i]) < 1e-11
+
+
+def test_oracle_failure_messages_follow_negfpy():
+    """The oracle's decimation separates overflow from finite blocks
+    ("numerically unstable") from NaN blocks ("non-finite values") as
+    negfpy does (tests/golden/dos_workflow.npz holds negfpy's messages)."""
+    import json
+
+    from tests.golden.make_golden import SR_FAILURE_ORDERS, sr_failure_blocks
+
+    ref = json.loads(str(np.load(GOLDEN / "dos_workflow.npz")["sr_failure_messages"]))
+    for n in SR_FAILURE_ORDERS:
+        for case, (d00, d01) in sr_failure_blocks(n).items():
+            with pytest.raises(O.OracleError) as info:
+                O.sancho_rubio(0.5, d00, d01, eta=1e-8)
+            assert ref[f"{case}_{n}"].split(": ", 1)[1].startswith(str(info.value).rstrip("."))
