@@ -99,13 +99,15 @@ __device__ __forceinline__ double block_sum(double v, double* red) {
 // Returns nonzero in every thread if any thread passed nonzero.
 __device__ __forceinline__ int block_any(int v) { return __syncthreads_or(v); }
 
-// The status of a decimation that met inf/nan in iteration `it` (an
-// inversion pivot, or the products and sums).  negfpy runs each iteration
-// under numpy's floating-point traps (core/surface_gf.py:40-56): an overflow
-// or invalid operation there is "numerically unstable", while inf/nan that
-// came in with the blocks pass through quietly and are "non-finite values".
-// Every iteration after the first starts from finite blocks, so only the
-// first can be the quiet case.  Every thread of the block calls this.
+// The status of a decimation whose products or sums of iteration `it` came
+// out non-finite.  negfpy runs each iteration under numpy's floating-point
+// traps (core/surface_gf.py:40-56): an overflow or invalid operation in the
+// products is "numerically unstable", while inf/nan that came in with the
+// blocks pass through quietly and are "non-finite values".  Every iteration
+// after the first starts from finite blocks, so only the first can be the
+// quiet case.  (An inversion that meets inf/nan stays kNonFinite: numpy's
+// inverse runs with the traps off and hands NaN on quietly.)  Every thread
+// of the block calls this.
 __device__ __forceinline__ int sr_failure_status(int it, int n, const double2* h00, const double2* h01,
                                                  const double2* h10, double2 z) {
   int bad = 0;

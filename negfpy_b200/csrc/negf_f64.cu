@@ -739,11 +739,13 @@ __global__ void __launch_bounds__(Geo<NP>::NTH, 1) sr_f64_kernel(SrArgs a) {
     f1 = pag;
     f2 = pbg;
     pa = pg;
-    if (block_any(bad)) { status = kNonFinite; break; }
+    if (block_any(bad)) {
+      status = sr_failure_status(it, n, h00, h01, h10, z);
+      break;
+    }
     const double emax = block_max(e2, red);
     if (emax < tol2) { converged = true; break; }
   }
-  if (status == kNonFinite) status = sr_failure_status(it, n, h00, h01, h10, z);
   if (status == kOk && !converged) {
     status = kMaxIter;
     it = a.maxiter;

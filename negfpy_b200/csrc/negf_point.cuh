@@ -125,7 +125,7 @@ static __device__ int sr_point(int n, int NP, const double2* h00, const double2*
       f2 = pag;
     }
     if (block_any(bad)) {
-      status = kNonFinite;
+      status = sr_failure_status(it, n, h00, h01, h10, z);
       break;
     }
     const double emax = block_max(e2, red);
@@ -134,7 +134,6 @@ static __device__ int sr_point(int n, int NP, const double2* h00, const double2*
       break;
     }
   }
-  if (status == kNonFinite) status = sr_failure_status(it, n, h00, h01, h10, z);
   if (status == kOk && !converged) {
     status = kMaxIter;
     it = maxiter;

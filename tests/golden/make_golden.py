@@ -312,6 +312,12 @@ STUDY_RUNS = [
                       "20260226_032511Z_phosphorene_p_zerostrain_transmission_x_area"),
     ("borophene_y", "borophene_b_2x1_pbe_2026q1/borophene_b_2x1_pbe/runs/"
                     "20260225_033229Z_borophene_b_2x1_pbe_transmission_y"),
+    ("stanene_y", "stanene_1l_orthogonal_2026q1/stanene_1l_orthogonal/runs/"
+                  "20260226_031515Z_stanene_1l_orthogonal_transmission_y_area"),
+    ("beta12_x", "borophene_b_beta12_2026q1/borophene_b_beta12/runs/"
+                 "20260226_034715Z_borophene_b_beta12_transmission_area"),
+    ("beta12_y", "borophene_b_beta12_2026q1/borophene_b_beta12/runs/"
+                 "20260226_035209Z_borophene_b_beta12_transmission_area_y"),
 ]
 
 

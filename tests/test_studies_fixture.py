@@ -5,11 +5,15 @@ surface GF; the fixture's ``sr_*`` entries are negfpy's _run_transmission on
 the same inputs with Sancho-Rubio, the reference the GPU test uses.
 
 Where the two surface GFs let the eta ladder pick the same eta at every k
-point, the values agree to 5e-9 max(|T|, 1) (2.3e-9 at most, at band edges).
-The one place they do not is TaN below 100 cm^-1 (omega indices 1-29, the
-256-point low mesh): there negfpy's Sancho-Rubio result at eta = 1e-8 is
-rejected at a few k points, which then take eta = 1e-7, while the QEP
-result never is."""
+point, the values agree to 5e-9 max(|T|, 1) (2.8e-9 at most, at band edges).
+They do not in two places:
+- TaN below 100 cm^-1 (omega indices 1-29, the 256-point low mesh): there
+  negfpy's Sancho-Rubio result at eta = 1e-8 is rejected at a few k points,
+  which then take eta = 1e-7, while the QEP result never is;
+- the beta-12 boron sheet along y (n = 90; omega indices 1-117): at
+  eta = 1e-8 negfpy's decimation overflows at most k points ("numerically
+  unstable"), the ladder moves them to 1e-7 ... 1e-5, and the values end up
+  as much as 49 % away from the QEP run's."""
 
 from __future__ import annotations
 
@@ -21,7 +25,7 @@ import pytest
 from tests.conftest import GOLDEN
 from tests.golden.make_golden import STUDY_RUNS, THERMAL_RUNS
 
-LADDER_DIFFERS = {"tan_x": list(range(1, 30))}
+LADDER_DIFFERS = {"tan_x": list(range(1, 30)), "beta12_y": list(range(1, 118))}
 
 
 @pytest.fixture(scope="module")
