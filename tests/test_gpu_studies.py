@@ -8,7 +8,8 @@ parameters to the k-averaged T(omega) and its eta records
 The reference values are negfpy's _run_transmission on the same inputs with
 the Sancho-Rubio surface GF (tests/test_studies_fixture.py ties them to the
 transmission.tsv files those runs wrote with the QEP surface GF).  Bound:
-1e-10 max(|T|, 1) per omega, and equal eta records.
+1e-10 max(|T|, 1) per omega (the beta-12 sheet along y excepted, see
+TOL_RUN), and equal eta records.
 """
 
 from __future__ import annotations
