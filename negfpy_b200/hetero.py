@@ -25,7 +25,6 @@ block gradients that the adjoint kernel provides.
 from __future__ import annotations
 
 from dataclasses import dataclass
-from itertools import product
 
 import numpy as np
 import torch

@@ -14,14 +14,12 @@ raise ``ValueError``.
 
 from __future__ import annotations
 
-from collections.abc import Callable
-
 import numpy as np
 import torch
 
 from . import _lib, engine
 from .surface_gf import check_method, raise_for_status
-from .types import Device1D, LeadBlocks, resolve_device, resolve_lead_blocks
+from .types import resolve_device, resolve_lead_blocks
 
 Array = np.ndarray
 
