@@ -23,3 +23,26 @@ def test_fcs_stage_checks(fix, bad, msg):
     cfg = FCS_CFGS["delta_conductance"]
     with pytest.raises(ValueError, match=msg):
         _run(fix, "si", {**cfg, "fcs": {**cfg["fcs"], **bad}})
+
+
+def test_stages_without_launches():
+    """Paths of the DOS and FCS stages that negfpy settles before any solve
+    (workflows/ifc_bulk.py:1290-1441, 1690-1784): a QEP surface-GF name is
+    refused, negative omegas are NaN without a failure record (all of them:
+    "DOS calculation failed for all omega points."), and omega <= 0 has zero
+    k moments."""
+    from negfpy_b200 import workflow as WF
+
+    km = {"low_cm1": 100.0, "low": {"kpoints": [(0.0,)]}, "high": {"kpoints": [(0.0,)]}}
+    with pytest.raises(NotImplementedError):
+        WF.run_dos({"solver": {"surface_gf_method": "generalized_eigen_svd"}}, lead=None, omegas=[-1.0], kmesh=km)
+    with pytest.raises(NotImplementedError):
+        WF.compute_fcs_k_moments({"solver": {}}, device=None, lead_left=None, lead_right=None, omegas=[0.0],
+                                 kmesh=km)
+    with pytest.raises(RuntimeError, match="DOS calculation failed for all omega points"):
+        WF.run_dos({"solver": {"surface_gf_method": "sr"}}, lead=None, omegas=[-1.0, -0.5], kmesh=km)
+    res = WF.compute_fcs_k_moments({"solver": {"surface_gf_method": "sancho_rubio"}}, device=None, lead_left=None,
+                                   lead_right=None, omegas=[-0.2, 0.0], kmesh=km)
+    assert res["t_mean"].tolist() == [0.0, 0.0] and res["t2_mean"].tolist() == [0.0, 0.0]
+    assert res["n_k_success"].tolist() == [0, 0] and res["omega_failures"] == []
+    assert np.isnan(res["eta_selected"]).all()
