@@ -115,10 +115,11 @@ int negf_rgf_transmission_f64(int n_dev, int n_lead_l, int n_lead_r, int n_layer
  * exits.  The first call on a device looks up that array's device address
  * (make it before any stream capture).  Calls share the array: calls whose
  * GPU work overlaps race and must not be issued concurrently.  Returns
- * NEGF_EUNSUPPORTED for block orders above 48 (the same limit as the
- * allocating entry point; the persistent grid is capped to what fits the
- * array), NEGF_EINVAL / NEGF_ECUDA as the other entry points.  Calls no
- * allocator.
+ * NEGF_EUNSUPPORTED for block orders above 48, which run only from shared
+ * memory here (the allocating form runs orders 49..256 on its global-
+ * workspace kernels); the persistent grid is capped to what fits the array.
+ * NEGF_EINVAL / NEGF_ECUDA as the other entry points, with the message in
+ * negf_last_error().  Calls no allocator.
  */
 int negf_rgf_transmission_f64_noalloc(int n_dev, int n_lead_l, int n_lead_r, int n_layers, int batch,
                                       const double* onsite, long long onsite_kstride, long long onsite_lstride,

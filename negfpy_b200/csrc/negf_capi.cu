@@ -22,6 +22,10 @@ inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s
 constexpr size_t kCounterBytes = 256;
 }  // namespace
 
+namespace negf {
+int record_error(int code, const char* msg) { return fail(code, msg); }
+}  // namespace negf
+
 extern "C" {
 
 int negf_get_version(void) { return NEGF_B200_ABI_VERSION; }

@@ -63,6 +63,9 @@ struct FullArgs {
 
 int padded_order(int n);
 const char* last_launch_error();  // message of the last failed launch on this thread
+// Records `msg` as the text negf_last_error() returns on this host thread and
+// returns `code`; for entry points defined outside negf_capi.cu.
+int record_error(int code, const char* msg);
 int sr_f64_launch(const SrArgs& a, cudaStream_t st);
 // Padded order np = padded_order(max(n, nl, nr)) selects the kernel variant.
 int rgf_f64_grid(int np);  // persistent grid size (blocks), 0 for the 1x1 path

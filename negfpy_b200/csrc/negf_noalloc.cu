@@ -35,14 +35,10 @@ __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
 std::mutex g_mu;
 void* g_scratch_addr[kMaxDevices] = {nullptr};
-// Failures are reported by return code only (see include/negf_b200.h); the
-// message is kept for a debugger.
-thread_local char g_noalloc_err[256] = "";
 
-int noalloc_fail(int code, const char* msg) {
-  snprintf(g_noalloc_err, sizeof(g_noalloc_err), "%s", msg);
-  return code;
-}
+// Failures go through the library's shared per-thread message, so
+// negf_last_error() describes them like those of every other entry point.
+int noalloc_fail(int code, const char* msg) { return negf::record_error(code, msg); }
 
 // Device address of the scratch array on the current device (looked up once).
 void* scratch_address(int* rc) {
@@ -56,9 +52,10 @@ void* scratch_address(int* rc) {
     void* p = nullptr;
     const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess || p == nullptr) {
-      snprintf(g_noalloc_err, sizeof(g_noalloc_err), "negf_rgf_transmission_f64_noalloc: cudaGetSymbolAddress: %s",
+      char msg[256];
+      snprintf(msg, sizeof(msg), "negf_rgf_transmission_f64_noalloc: cudaGetSymbolAddress: %s",
                cudaGetErrorString(e));
-      *rc = NEGF_ECUDA;
+      *rc = noalloc_fail(NEGF_ECUDA, msg);
       return nullptr;
     }
     g_scratch_addr[dev] = p;
@@ -92,10 +89,9 @@ int negf_rgf_transmission_f64_noalloc(int n_dev, int n_lead_l, int n_lead_r, int
   const int np = negf::padded_order(max3i(n_dev, n_lead_l, n_lead_r));
   if (np == 0)
     return noalloc_fail(NEGF_EUNSUPPORTED, "negf_rgf_transmission_f64_noalloc: block order above 48 is not supported");
-  // Scratch per persistent block: two n_dev x n_dev complex self-energies.
+  // Scratch per persistent block: two n_dev x n_dev complex self-energies,
+  // at most 72 KiB for n_dev <= 48, so at least 227 blocks fit the array.
   const size_t per_block = size_t(2) * n_dev * n_dev * 16;
-  if (np != 1 && kCounterBytes + per_block > kNoAllocScratchBytes)
-    return noalloc_fail(NEGF_EUNSUPPORTED, "negf_rgf_transmission_f64_noalloc: scratch need exceeds the 16 MiB array");
   int rc = 0;
   void* base = scratch_address(&rc);
   if (!base) return rc;
@@ -104,8 +100,13 @@ int negf_rgf_transmission_f64_noalloc(int n_dev, int n_lead_l, int n_lead_r, int
   if (np != 1) {
     grid = negf::rgf_f64_grid(np);
     if (grid <= 0) return noalloc_fail(NEGF_ECUDA, "negf_rgf_transmission_f64_noalloc: occupancy query failed");
+    // The kernel takes work from a counter, so any grid >= 1 is valid.  On a
+    // 148-SM B200 the occupancy grid stays below the fit: registers and
+    // shared memory allow 1 block per SM at padded order 48, 2 at 32 and at
+    // most 8 at 16 (148, 296 and 1184 blocks), against a fit of at least
+    // 227, 511 and 2047 blocks.  The cap only acts on GPUs with more SMs.
     const size_t fit = (kNoAllocScratchBytes - kCounterBytes) / per_block;
-    if ((size_t)grid > fit) grid = (int)fit;  // the kernel takes work from a counter, any grid >= 1 is valid
+    if ((size_t)grid > fit) grid = (int)fit;
   }
   negf::RgfArgs a;
   a.n = n_dev;

@@ -4,12 +4,16 @@ negf_rgf_transmission_f64_noalloc exists for callers that cannot allocate
 device memory when they call the library (a host program that fixed its GPU
 memory budget up front, or a binding without a CUDA allocator): it keeps its
 scratch in a static device array instead of a caller workspace.  This test
-calls it through the C ABI twice in a row -- the second call reuses the
-array and must not see the first call's leftovers -- and compares each
-result with negf_rgf_transmission_f64 on the same inputs, to the FP64
-tolerance of the parity tests (1e-10 relative, floor 1).  The file is named
-to be collected last so that a run stopping at the first failure has already
-run every other test; it also passes on its own in a fresh process.
+calls it through the C ABI twice in a row on two different systems -- an
+order-48 slab with 48 points, then an order-24 slab with fewer points -- and
+compares each result with negf_rgf_transmission_f64 on the same inputs, to
+the FP64 tolerance of the parity tests (1e-10 relative, floor 1).  The second
+call reuses the array: self-energies left over from the first call, or a
+work counter that was not cleared (it would stand above the second call's
+point count and leave its points unsolved, NaN), show up as a mismatch.  The
+file is named to be collected last so that a run stopping at the first
+failure has already run every other test; it also passes on its own in a
+fresh process.
 """
 
 import numpy as np
@@ -23,8 +27,8 @@ pytestmark = pytest.mark.gpu
 TOL = 1e-10
 
 
-def _system():
-    wl = W.subsample(W.slab_workload(n_omega=64, n_k=8, n_layers=6), list(range(0, 64, 4)), [0, 3, 5])
+def _system(nz: int, omega_idx, k_idx):
+    wl = W.subsample(W.slab_workload(n_omega=64, n_k=8, n_layers=6, nz=nz), omega_idx, k_idx)
     s = engine.StackedSystem.from_arrays(wl.lead_l, wl.lead_l, wl.onsite, wl.coupling, wl.n_layers)
     dev = _lib.require_cuda()
     K, Wn = len(wl.kpoints), len(wl.omegas)
@@ -59,16 +63,19 @@ def _noalloc(lib, s, om, eta, ki, sr):
 
 def test_noalloc_matches_allocating_entry_point_on_two_calls():
     lib = _lib.load()
-    s, om, eta, ki, sr = _system()
-    T_ref, st_ref = engine.rgf_transmission(s.onsite, s.coupling, s.n_layers, s.vl, s.vr, sr["g"], sr["g"], om, eta,
-                                            ki, sr["status"])
-    T_ref, st_ref = T_ref.cpu().numpy(), st_ref.cpu().numpy()
-    assert np.all(st_ref == 0)
-    for _ in range(2):
+    cases = [(8, list(range(0, 64, 4)), [0, 3, 5]),  # order 48, 48 points
+             (4, [7, 21, 40, 55], [1, 6])]  # order 24, 8 points
+    for nz, wi, ki_sel in cases:
+        s, om, eta, ki, sr = _system(nz, wi, ki_sel)
+        assert s.n == 6 * nz
+        T_ref, st_ref = engine.rgf_transmission(s.onsite, s.coupling, s.n_layers, s.vl, s.vr, sr["g"], sr["g"], om,
+                                                eta, ki, sr["status"])
+        T_ref, st_ref = T_ref.cpu().numpy(), st_ref.cpu().numpy()
+        assert np.all(st_ref == 0)
         T, st = _noalloc(lib, s, om, eta, ki, sr)
         assert np.array_equal(st, st_ref)
         err = np.abs(T - T_ref) / np.maximum(np.abs(T_ref), 1.0)
-        assert err.max() <= TOL, err.max()
+        assert err.max() <= TOL, (s.n, err.max())
 
 
 def test_noalloc_rejects_unsupported_block_order():
@@ -80,3 +87,5 @@ def test_noalloc_rejects_unsupported_block_order():
         x.data_ptr(), 0, x.data_ptr(), 0, None, x.data_ptr(), x.data_ptr(), None, x.data_ptr(), None,
         torch.cuda.current_stream().cuda_stream)
     assert rc == -2  # NEGF_EUNSUPPORTED
+    msg = lib.negf_last_error().decode()
+    assert msg.startswith("negf_rgf_transmission_f64_noalloc") and "48" in msg, msg
