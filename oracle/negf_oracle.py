@@ -72,6 +72,22 @@ def sancho_rubio(omega, d00, d01, d10=None, eta=1e-8, tol=1e-12, maxiter=200):
     raise OracleError("Sancho-Rubio decimation did not converge within maxiter.")
 
 
+def surface_residual(omega, d00, d01, d10=None, eta=1e-8, tol=1e-12, maxiter=200):
+    """How well the decimated surface GF solves its own fixed point.
+
+    Runs ``sancho_rubio`` (``core/surface_gf.py:18-81``) and returns
+    max|g - (z - d00 - d01 g d10)^-1| / max|g|.  At ordinary points this is
+    ~1e-13; near band edges the decimation's cancellations leave it at
+    1e-8 ... 1e-5, and there rounding alone moves negfpy's T by about as much.
+    """
+    g, _ = sancho_rubio(omega, d00, d01, d10, eta, tol, maxiter)
+    z = (omega + 1j * eta) ** 2
+    d10 = np.conj(d01).T if d10 is None else d10
+    n = d00.shape[0]
+    fix = np.linalg.inv(z * np.eye(n, dtype=np.complex128) - d00 - d01 @ g @ d10)
+    return float(np.max(np.abs(g - fix)) / np.max(np.abs(g)))
+
+
 def qep_surface_gf(omega, d00, d01, d10=None, eta=1e-8, unit_circle_tol=1e-10):
     """Generalised-eigen (QEP) surface GF, ``core/surface_gf.py:84-133``.
 
@@ -242,6 +258,14 @@ def _pool_task(args):
         return float("nan")
 
 
+def _residual_task(args):
+    try:
+        d00, d01, d10 = args["lead_l"]
+        return surface_residual(args["omega"], d00, d01, d10, args["eta"])
+    except (OracleError, np.linalg.LinAlgError):
+        return float("nan")
+
+
 def make_pool(processes):
     """Spawn pool with one BLAS thread per worker, as negfpy's process backend
     (``workflows/ifc_bulk.py:1229-1253``, ``:621-670``); spawn, not fork, so it
@@ -365,3 +389,11 @@ def device_green_point(omega, onsite, coupling, lead_l, lead_r, eta=1e-8, eta_de
     sig_l[np.ix_(il, il)] = sl
     sig_r[np.ix_(ir, ir)] = sr
     return g, sig_l, sig_r
+
+
+def surface_residual_points(wl, pairs, pool=None):
+    """Left-lead ``surface_residual`` for (omega_index, k_index) pairs of a workload."""
+    args = [workload_point_args(wl, wi, ki) for wi, ki in pairs]
+    if pool is None:
+        return np.array([_residual_task(a) for a in args])
+    return np.array(pool.map(_residual_task, args, chunksize=1))

@@ -1,9 +1,9 @@
 """Generate the golden vectors of the NEGF path by running negfpy itself.
 
-Run from the repository root, with negfpy importable (its ``src`` directory on
-PYTHONPATH; the default below is where this build's reference checkout lives):
+Run from the repository root and name negfpy's ``src`` directory, either with
+``--ref`` or in the NEGFPY_SRC environment variable:
 
-    python tests/golden/make_golden.py [--ref /path/to/negfpy/src]
+    python tests/golden/make_golden.py --ref /path/to/negfpy/src
 
 Inputs are the seeded synthetic workloads of ``negfpy_b200.workloads`` (their
 blocks are stored with the outputs, so the fixtures do not depend on the
@@ -609,10 +609,13 @@ def sr_failure_blocks(n: int) -> dict:
 
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference/src")
+    ap.add_argument("--ref", default=os.environ.get("NEGFPY_SRC"),
+                    help="negfpy's src directory (default: $NEGFPY_SRC)")
     ap.add_argument("--only", choices=["thermal", "green", "workflow", "interface", "dos", "studies", "fcs", "dos_workflow"], default=None,
                     help="write one fixture file only")
     args = ap.parse_args()
+    if not args.ref:
+        ap.error("name negfpy's src directory with --ref or NEGFPY_SRC")
     sys.path.insert(0, args.ref)
     if args.only == "thermal":
         thermal(OUT)
