@@ -179,6 +179,37 @@ int negf_rgf_transmission_mixed(int n_dev, int n_lead_l, int n_lead_r, int n_lay
                                 double* t_out, int* status_out, void* workspace, size_t workspace_bytes,
                                 void* stream);
 
+/* Workspace bytes negf_rgf_transmission_refined needs (0 on a bad size). */
+size_t negf_rgf_refined_workspace_bytes(int n_dev, int n_lead_l, int n_lead_r, int n_layers);
+
+/*
+ * Batched device solve and transmission with FP64 accuracy from FP32
+ * factors: the arguments, outputs and status codes of
+ * negf_rgf_transmission_f64 (replacing negfpy core/negf.py:72-357, whose
+ * SuperLU solve of A X = E_R, core/negf.py:346-353, this refines), plus
+ * tol, max_steps and steps_out.  The block LU factors of A come from an FP32
+ * sweep (3 x TF32 tensor-core products, FP32 Gauss-Jordan); the right-contact
+ * block column X is then refined: R = E_R - A X in FP64, A d = R solved with
+ * the FP32 factors, X += d.  It stops after the first step k whose relative
+ * correction of X_0 = G_{0,L-1}, nu_k, satisfies nu_k^2 / nu_{k-1} <= tol
+ * (nu_0 = 1).  A point whose correction fails to halve from one step to the
+ * next, or that does not converge within max_steps, reports
+ * NEGF_REFINE_FAIL; a singular or non-finite FP32 pivot NEGF_SINGULAR /
+ * NEGF_NONFINITE.  The caller re-solves those points with
+ * negf_rgf_transmission_f64.  Self-energies, broadenings and the trace are
+ * FP64.  steps_out[p] (may be NULL): refinement steps taken.  Block orders
+ * 1..256.
+ */
+int negf_rgf_transmission_refined(int n_dev, int n_lead_l, int n_lead_r, int n_layers, int batch,
+                                  const double* onsite, long long onsite_kstride, long long onsite_lstride,
+                                  const double* coupling, long long coupling_kstride, long long coupling_lstride,
+                                  const double* v_left, long long v_left_kstride, const double* v_right,
+                                  long long v_right_kstride, const double* g_left, long long g_left_pstride,
+                                  const double* g_right, long long g_right_pstride, const int* k_index,
+                                  const double* omega, const double* eta_device, const int* lead_status,
+                                  double tol, int max_steps, double* t_out, int* status_out, int* steps_out,
+                                  void* workspace, size_t workspace_bytes, void* stream);
+
 /* Workspace bytes negf_rgf_adjoint_f64 needs (0 on a bad size). */
 size_t negf_adjoint_workspace_bytes(int n_dev, int n_lead_l, int n_lead_r, int n_layers);
 
@@ -204,6 +235,58 @@ int negf_rgf_adjoint_f64(int n_dev, int n_lead_l, int n_lead_r, int n_layers, in
                          const double* eta_device, const int* lead_status, const double* weight, double* grad_onsite,
                          double* grad_coupling, double* t_out, int* status_out, void* workspace,
                          size_t workspace_bytes, void* stream);
+
+/*
+ * negf_rgf_adjoint_f64 that also writes, per point, the weighted adjoint of
+ * each contact self-energy (no counterpart in negfpy; it differentiates
+ * core/negf.py:72-116, 306-357 with respect to Sigma_L and Sigma_R):
+ *   sigma_adj_left[p]  = weight[p] (X_00 + i G Gamma_R G^H)              ([batch][n][n])
+ *   sigma_adj_right[p] = weight[p] (X_{L-1,L-1} + i G^H Gamma_L G)
+ * with G = G_{0,L-1}, so that dT = 2 Re Tr[dSigma_L sigma_adj_left] + ...
+ * (Sigma enters both A and Gamma).  Either output may be NULL, not both.
+ * Points that fail are not written (the caller zeroes the outputs).
+ * Workspace as negf_rgf_adjoint_f64 (negf_adjoint_workspace_bytes).
+ */
+int negf_rgf_adjoint_sigma_f64(int n_dev, int n_lead_l, int n_lead_r, int n_layers, int batch, const double* onsite,
+                               long long onsite_kstride, long long onsite_lstride, const double* coupling,
+                               long long coupling_kstride, long long coupling_lstride, const double* v_left,
+                               long long v_left_kstride, const double* v_right, long long v_right_kstride,
+                               const double* g_left, long long g_left_pstride, const double* g_right,
+                               long long g_right_pstride, const int* k_index, const double* omega,
+                               const double* eta_device, const int* lead_status, const double* weight,
+                               double* grad_onsite, double* grad_coupling, double* sigma_adj_left,
+                               double* sigma_adj_right, double* t_out, int* status_out, void* workspace,
+                               size_t workspace_bytes, void* stream);
+
+/* Workspace bytes negf_sgf_adjoint_f64 needs (0 on a bad size). */
+size_t negf_sgf_adjoint_workspace_bytes(int n_lead, int n_dev);
+
+/*
+ * Adjoint of the surface Green's function and of Sigma = V g V^H, FP64 (no
+ * counterpart in negfpy; it differentiates the fixed point that
+ * core/surface_gf.py:18-81 decimates to, g = (z - H00 - H01 g H10)^-1, and
+ * core/negf.py:72-97, Sigma = V g V^H, implicitly: nothing is differentiated
+ * through the decimation sweeps).  Per point p with lead set k = k_index[p]:
+ * g[p] (n_lead x n_lead, from negf_sgf_sr_f64), the coupling V at
+ * v + k*v_kstride (n_dev x n_lead) and sigma_adj[p] (n_dev x n_dev, from
+ * negf_rgf_adjoint_sigma_f64).  It solves Lam - Q Lam P = V^H X V with
+ * P = g H01, Q = H10 g by doubling (until max(|Q^(2^j)|, |P^(2^j)|) < tol,
+ * at most maxiter doublings; iters_out) and ADDS, in the convention
+ * dT = 2 Re Tr[dH X]:
+ *   grad_h00[k] += g Lam g,  grad_h01[k] += g H10 g Lam g,
+ *   grad_h10[k] += g Lam g H01 g      (h10 NULL: H10 = H01^H, and this
+ *                                      term's ^H is added to grad_h01),
+ *   grad_v[k]   += g V^H X + g^H V^H X^H     ([K or 1][n_lead][n_dev]).
+ * The caller zeroes the accumulators.  Status per point: NEGF_MAXITER,
+ * NEGF_NONFINITE; points with nonzero lead_status are skipped.  Orders
+ * 1..256.
+ */
+int negf_sgf_adjoint_f64(int n_lead, int n_dev, int batch, const double* h01, const double* h10,
+                         long long lead_stride, const double* v, long long v_kstride, const double* g,
+                         long long g_pstride, const double* sigma_adj, const int* k_index, const int* lead_status,
+                         double tol, int maxiter, double* grad_h00, double* grad_h01, double* grad_h10,
+                         double* grad_v, int* iters_out, int* status_out, void* workspace, size_t workspace_bytes,
+                         void* stream);
 
 /*
  * One lead/device/lead system of an uneven batch (negf_batch_transmission).

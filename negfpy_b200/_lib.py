@@ -50,6 +50,12 @@ _SIGNATURES = {
         [_I, _I, _I, _I, _I, _P, _LL, _LL, _P, _LL, _LL, _P, _LL, _P, _LL, _P, _LL, _P, _LL, _P, _P, _P, _P, _P,
          _P, _P, _SZ, _P],
     ),
+    "negf_rgf_refined_workspace_bytes": (_SZ, [_I, _I, _I, _I]),
+    "negf_rgf_transmission_refined": (
+        _I,
+        [_I, _I, _I, _I, _I, _P, _LL, _LL, _P, _LL, _LL, _P, _LL, _P, _LL, _P, _LL, _P, _LL, _P, _P, _P, _P, _D,
+         _I, _P, _P, _P, _P, _SZ, _P],
+    ),
     "negf_batch_max_grid": (_I, [_I, _I, _I]),
     "negf_batch_workspace_bytes": (_SZ, [_I, _I, _I, _I]),
     "negf_batch_system_bytes": (_SZ, []),
@@ -67,6 +73,16 @@ _SIGNATURES = {
         _I,
         [_I, _I, _I, _I, _I, _P, _LL, _LL, _P, _LL, _LL, _P, _LL, _P, _LL, _P, _LL, _P, _LL, _P, _P, _P, _P, _P,
          _P, _P, _P, _P, _P, _SZ, _P],
+    ),
+    "negf_rgf_adjoint_sigma_f64": (
+        _I,
+        [_I, _I, _I, _I, _I, _P, _LL, _LL, _P, _LL, _LL, _P, _LL, _P, _LL, _P, _LL, _P, _LL, _P, _P, _P, _P, _P,
+         _P, _P, _P, _P, _P, _P, _P, _SZ, _P],
+    ),
+    "negf_sgf_adjoint_workspace_bytes": (_SZ, [_I, _I]),
+    "negf_sgf_adjoint_f64": (
+        _I,
+        [_I, _I, _I, _P, _P, _LL, _P, _LL, _P, _LL, _P, _P, _P, _D, _I, _P, _P, _P, _P, _P, _P, _P, _SZ, _P],
     ),
     "negf_kavg_f64": (_I, [_P, _I, _I, _P, _P]),
     "negf_heat_current_f64": (_I, [_P, _P, _I, _I, _D, _D, _P, _P]),

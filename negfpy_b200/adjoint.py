@@ -169,6 +169,162 @@ class HeteroKappaProblem(DeviceSolve):
         return self.kappa_of_t(T), dth, dm
 
 
+    # ----------------------------------------------- leads as variables too
+    def leads(self, masses: torch.Tensor | None = None, phi_a: torch.Tensor | None = None,
+              phi_b: torch.Tensor | None = None):
+        """Lead blocks and contact couplings as torch tensors of the current
+        parameters: (lead A, lead B, V_L [K, n, n_A], V_R [K, n, n_B]);
+        V_L holds lead A's d10 on the device rows of layer 0 and V_R is lead
+        B's d01, the couplings ``__init__`` builds from the fixed leads."""
+        dev = self.om.device
+        mdl = self.model
+        la = mdl.lead_blocks_torch("A", self.kpoints, phi_a, masses, device=dev)
+        lb = mdl.lead_blocks_torch("B", self.kpoints, phi_b, masses, device=dev)
+        rows = torch.as_tensor(mdl.contact_left_indices(), device=dev)
+        vl = torch.zeros((self.K, mdl.n, mdl.n_a), dtype=torch.complex128, device=dev)
+        vl = vl.index_copy(1, rows, la["d10"])
+        return la, lb, vl, lb["d01"]
+
+    def _points(self):
+        return PointGrid(self.omega, self.eta, self.ki, self.W, self.K, self.L)
+
+    def kappa_full(self, theta: torch.Tensor, masses: torch.Tensor | None = None, phi_a: torch.Tensor | None = None,
+                   phi_b: torch.Tensor | None = None) -> float:
+        """kappa with every part rebuilt from the parameters: both leads'
+        blocks and surface GFs (decimated again), the couplings and the
+        device (the forward of ``kappa_and_grad_all``)."""
+        with torch.no_grad():
+            on, cp = self.model.blocks(theta, self.kpoints, masses, phi_a=phi_a, phi_b=phi_b)
+            la, lb, vl, vr = self.leads(masses, phi_a, phi_b)
+            T = transport(on, cp, vl, vr, la["d00"], la["d01"], lb["d00"], lb["d01"], self._points(), grad=False)[0]
+        return float(self.kappa_of_t(T))
+
+    def kappa_and_grad_all(self, theta: torch.Tensor, masses: torch.Tensor | None = None,
+                           phi_a: torch.Tensor | None = None, phi_b: torch.Tensor | None = None):
+        """(kappa, dkappa/dtheta, dkappa/dmasses, dkappa/dphi_a, dkappa/dphi_b)
+        with the leads differentiated too: both decimations, one device
+        adjoint launch that also returns the contact self-energy adjoints, one
+        surface-GF adjoint launch per lead, then one autograd pass through the
+        device and lead block builders."""
+        dev = self.om.device
+        mdl = self.model
+
+        def leaf(x, default):
+            x = torch.as_tensor(default, device=dev) if x is None else x
+            return x.detach().clone().to(device=dev, dtype=torch.float64).requires_grad_(True)
+
+        th = leaf(theta, mdl.theta0)
+        m = leaf(masses, mdl.mass)
+        pa = leaf(phi_a, mdl.phi0_a)
+        pb = leaf(phi_b, mdl.phi0_b)
+        on, cp = mdl.blocks(th, self.kpoints, m, phi_a=pa, phi_b=pb)
+        la, lb, vl, vr = self.leads(m, pa, pb)
+        w = (self.w_kappa[:, None] / self.K).expand(self.W, self.K)
+        T, grads = transport_vjp(on, cp, vl, vr, la["d00"], la["d01"], lb["d00"], lb["d01"], self._points(), w)
+        outs = [on, cp, vl, vr, la["d00"], la["d01"], lb["d00"], lb["d01"]]
+        d = torch.autograd.grad(outs, [th, m, pa, pb], list(grads), allow_unused=True)
+        d = [torch.zeros_like(x) if g is None else g for g, x in zip(d, (th, m, pa, pb))]
+        return (self.kappa_of_t(T), *d)
+
+
+class PointGrid:
+    """The (omega, k) points of a solve: omega-major, ``W`` x ``K``, device of ``L`` layers."""
+
+    def __init__(self, omega, eta, ki, W, K, L):
+        self.omega, self.eta, self.ki, self.W, self.K, self.L = omega, eta, ki, W, K, L
+
+
+def _x_to_grad(x: torch.Tensor) -> torch.Tensor:
+    """torch's gradient of a real loss from its adjoint X in dLoss = 2 Re Tr[dY X]: 2 conj(X^T)."""
+    return 2.0 * x.conj().transpose(-1, -2)
+
+
+def transport(onsite, coupling, vl, vr, l_d00, l_d01, r_d00, r_d01, pts: PointGrid, grad: bool = False,
+              tol: float = 1e-12, maxiter: int = 200):
+    """T[W, K] of a layer-resolved device between two leads given as blocks
+    (d10 = d01^H): decimation of both leads, then the device solve.  Returns
+    (T, (g_l, g_r, lead_status))."""
+    g_l, g_r, lst = _decimate(l_d00, l_d01, r_d00, r_d01, pts, tol, maxiter)
+    T, st = engine.rgf_transmission(onsite.detach().contiguous(), coupling.detach().contiguous(), pts.L,
+                                    vl.detach().contiguous(), vr.detach().contiguous(), g_l, g_r, pts.omega,
+                                    pts.eta, pts.ki, lst)
+    bad = int((st != 0).sum())
+    if bad:
+        raise RuntimeError(f"device solve failed at {bad} of {st.numel()} (omega, k) points")
+    return T.reshape(pts.W, pts.K), (g_l, g_r, lst)
+
+
+def transport_vjp(onsite, coupling, vl, vr, l_d00, l_d01, r_d00, r_d01, pts: PointGrid, weight: torch.Tensor,
+                  g=None, tol: float = 1e-12, maxiter: int = 200):
+    """(T[W, K], torch gradients of sum weight*T with respect to onsite,
+    coupling, vl, vr, l_d00, l_d01, r_d00, r_d01).  The surface GFs ``g`` =
+    (g_l, g_r, lead_status) are decimated here unless given; the device
+    adjoint recomputes its sweeps and returns the contact self-energy
+    adjoints, which the surface-GF adjoint kernel turns into lead-block and
+    coupling gradients (the d10 = d01^H part folded into d01)."""
+    if g is None:
+        g = _decimate(l_d00, l_d01, r_d00, r_d01, pts, tol, maxiter)
+    g_l, g_r, lst = g
+    w = weight.reshape(-1).to(device=pts.omega.device, dtype=torch.float64).contiguous()
+    T, st, x_on, x_cp, xs_l, xs_r = engine.rgf_adjoint(onsite.detach().contiguous(), coupling.detach().contiguous(),
+                                                       pts.L, vl.detach().contiguous(), vr.detach().contiguous(),
+                                                       g_l, g_r, pts.omega, pts.eta, pts.ki, lst, w, want_sigma=True)
+    bad = int((st != 0).sum())
+    if bad:
+        raise RuntimeError(f"device solve failed at {bad} of {st.numel()} (omega, k) points")
+    al = engine.sgf_adjoint(l_d01.detach(), None, vl.detach(), g_l, xs_l, pts.ki, lst, tol, maxiter)
+    ar = engine.sgf_adjoint(r_d01.detach(), None, vr.detach(), g_r, xs_r, pts.ki, lst, tol, maxiter)
+    for a in (al, ar):
+        nb = int((a["status"] != 0).sum())
+        if nb:
+            raise RuntimeError(f"surface-GF adjoint failed at {nb} of {a['status'].numel()} points")
+    grads = (_x_to_grad(x_on), _x_to_grad(x_cp), _x_to_grad(al["v"]), _x_to_grad(ar["v"]), _x_to_grad(al["h00"]),
+             _x_to_grad(al["h01"]), _x_to_grad(ar["h00"]), _x_to_grad(ar["h01"]))
+    return T.reshape(pts.W, pts.K), grads
+
+
+def _decimate(l_d00, l_d01, r_d00, r_d01, pts, tol, maxiter):
+    rl = engine.sgf_sr(l_d00.detach().contiguous(), l_d01.detach().contiguous(), None, pts.omega, pts.eta, pts.ki,
+                       tol, maxiter)
+    rr = engine.sgf_sr(r_d00.detach().contiguous(), r_d01.detach().contiguous(), None, pts.omega, pts.eta, pts.ki,
+                       tol, maxiter)
+    return rl["g"], rr["g"], torch.where(rl["status"] != 0, rl["status"], rr["status"]).contiguous()
+
+
+class TransportFunction(torch.autograd.Function):
+    """T[W, K] = TransportFunction.apply(onsite, coupling, vl, vr, l_d00,
+    l_d01, r_d00, r_d01, points): the whole solve -- both leads decimated from
+    their blocks (d10 = d01^H), the device between them -- differentiable in
+    every block.  The forward keeps the surface GFs (one n x n matrix per
+    point and lead); the backward recomputes the device sweeps inside the
+    adjoint kernel and differentiates the surface GFs implicitly through
+    their fixed point."""
+
+    @staticmethod
+    def forward(ctx, onsite, coupling, vl, vr, l_d00, l_d01, r_d00, r_d01, pts: PointGrid):
+        T, g = transport(onsite, coupling, vl, vr, l_d00, l_d01, r_d00, r_d01, pts)
+        ctx.pts, ctx.g = pts, g
+        ctx.save_for_backward(onsite.detach(), coupling.detach(), vl.detach(), vr.detach(), l_d00.detach(),
+                              l_d01.detach(), r_d00.detach(), r_d01.detach())
+        return T
+
+    @staticmethod
+    def backward(ctx, grad_t):
+        blocks = ctx.saved_tensors
+        _, grads = transport_vjp(*blocks, ctx.pts, grad_t, g=ctx.g)
+        return (*grads, None)
+
+
+def kappa_all(theta: torch.Tensor, problem: HeteroKappaProblem, masses: torch.Tensor | None = None,
+              phi_a: torch.Tensor | None = None, phi_b: torch.Tensor | None = None) -> torch.Tensor:
+    """kappa in W/K through ``TransportFunction``: differentiable in theta, the
+    masses and the two material tables, leads included."""
+    on, cp = problem.model.blocks(theta, problem.kpoints, masses, phi_a=phi_a, phi_b=phi_b)
+    la, lb, vl, vr = problem.leads(masses, phi_a, phi_b)
+    T = TransportFunction.apply(on, cp, vl, vr, la["d00"], la["d01"], lb["d00"], lb["d01"], problem._points())
+    return problem.kappa_of_t(T)
+
+
 def kappa(theta: torch.Tensor, problem: HeteroKappaProblem, masses: torch.Tensor | None = None) -> torch.Tensor:
     """kappa(T) in W/K, differentiable in theta (and masses) through ``TransmissionFunction``."""
     on, cp = problem.blocks(theta, masses)

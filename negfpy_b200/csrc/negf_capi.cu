@@ -246,6 +246,78 @@ int negf_rgf_transmission_mixed(int n_dev, int n_lead_l, int n_lead_r, int n_lay
   return 0;
 }
 
+size_t negf_rgf_refined_workspace_bytes(int n_dev, int n_lead_l, int n_lead_r, int n_layers) {
+  if (n_dev <= 0 || n_lead_l <= 0 || n_lead_r <= 0 || n_layers <= 0) return 0;
+  const int np = negf::mixed_order(max3(n_dev, n_lead_l, n_lead_r));
+  if (np == 0) return 0;
+  const int grid = negf::rgf_refine_grid(np);
+  if (grid <= 0) return 0;
+  return kCounterBytes + negf::rgf_refine_ws_bytes(np, n_dev, n_layers, grid);
+}
+
+int negf_rgf_transmission_refined(int n_dev, int n_lead_l, int n_lead_r, int n_layers, int batch,
+                                  const double* onsite, long long onsite_kstride, long long onsite_lstride,
+                                  const double* coupling, long long coupling_kstride, long long coupling_lstride,
+                                  const double* v_left, long long v_left_kstride, const double* v_right,
+                                  long long v_right_kstride, const double* g_left, long long g_left_pstride,
+                                  const double* g_right, long long g_right_pstride, const int* k_index,
+                                  const double* omega, const double* eta_device, const int* lead_status,
+                                  double tol, int max_steps, double* t_out, int* status_out, int* steps_out,
+                                  void* workspace, size_t workspace_bytes, void* stream) {
+  if (n_dev <= 0 || n_lead_l <= 0 || n_lead_r <= 0 || n_layers <= 0 || batch < 0)
+    return fail(NEGF_EINVAL, "negf_rgf_transmission_refined: sizes must be positive");
+  if (!onsite || !v_left || !v_right || !g_left || !g_right || !omega || !eta_device || !t_out)
+    return fail(NEGF_EINVAL, "negf_rgf_transmission_refined: null pointer");
+  if (n_layers > 1 && !coupling) return fail(NEGF_EINVAL, "negf_rgf_transmission_refined: null coupling");
+  if (onsite_kstride < 0 || onsite_lstride < 0 || coupling_kstride < 0 || coupling_lstride < 0 ||
+      v_left_kstride < 0 || v_right_kstride < 0 || g_left_pstride < 0 || g_right_pstride < 0)
+    return fail(NEGF_EINVAL, "negf_rgf_transmission_refined: negative stride");
+  if (!(tol > 0.0) || max_steps <= 0)
+    return fail(NEGF_EINVAL, "negf_rgf_transmission_refined: tol and max_steps must be positive");
+  const int np = negf::mixed_order(max3(n_dev, n_lead_l, n_lead_r));
+  if (np == 0) return fail(NEGF_EUNSUPPORTED, "negf_rgf_transmission_refined: block order above 256");
+  const int grid = negf::rgf_refine_grid(np);
+  if (grid <= 0) return cuda_fail("negf_rgf_transmission_refined: occupancy query");
+  if (!workspace || workspace_bytes < kCounterBytes + negf::rgf_refine_ws_bytes(np, n_dev, n_layers, grid))
+    return fail(NEGF_EINVAL, "negf_rgf_transmission_refined: workspace missing or too small");
+  if (batch == 0) return 0;
+  negf::RgfArgs a;
+  a.n = n_dev;
+  a.nl = n_lead_l;
+  a.nr = n_lead_r;
+  a.L = n_layers;
+  a.batch = batch;
+  a.D = reinterpret_cast<const double2*>(onsite);
+  a.d_ks = onsite_kstride;
+  a.d_ls = onsite_lstride;
+  a.C = reinterpret_cast<const double2*>(coupling ? coupling : onsite);
+  a.c_ks = coupling_kstride;
+  a.c_ls = coupling_lstride;
+  a.VL = reinterpret_cast<const double2*>(v_left);
+  a.vl_ks = v_left_kstride;
+  a.VR = reinterpret_cast<const double2*>(v_right);
+  a.vr_ks = v_right_kstride;
+  a.gL = reinterpret_cast<const double2*>(g_left);
+  a.gl_ps = g_left_pstride;
+  a.gR = reinterpret_cast<const double2*>(g_right);
+  a.gr_ps = g_right_pstride;
+  a.kidx = k_index;
+  a.omega = omega;
+  a.eta_dev = eta_device;
+  a.lead_status = lead_status;
+  a.T_out = t_out;
+  a.status_out = status_out;
+  a.counter = reinterpret_cast<unsigned int*>(workspace);
+  a.sigma_ws = nullptr;
+  cudaStream_t st = as_stream(stream);
+  if (cudaMemsetAsync(workspace, 0, sizeof(unsigned int), st) != cudaSuccess)
+    return cuda_fail("negf_rgf_transmission_refined: counter reset");
+  if (negf::rgf_refine_launch(a, np, grid, static_cast<char*>(workspace) + kCounterBytes, tol, max_steps,
+                              steps_out, st) != 0)
+    return cuda_fail("negf_rgf_transmission_refined");
+  return 0;
+}
+
 int negf_batch_max_grid(int max_order, int precision, int blocks_per_sm) {
   if (max_order <= 0 || max_order > 256 || (precision != 0 && precision != 1)) return 0;
   if (blocks_per_sm != 1 && blocks_per_sm != 2) return 0;
@@ -379,30 +451,46 @@ size_t negf_adjoint_workspace_bytes(int n_dev, int n_lead_l, int n_lead_r, int n
   return kCounterBytes + negf::grad_ws_bytes(np, n_dev, n_layers, grid);
 }
 
-int negf_rgf_adjoint_f64(int n_dev, int n_lead_l, int n_lead_r, int n_layers, int batch, const double* onsite,
-                         long long onsite_kstride, long long onsite_lstride, const double* coupling,
-                         long long coupling_kstride, long long coupling_lstride, const double* v_left,
-                         long long v_left_kstride, const double* v_right, long long v_right_kstride,
-                         const double* g_left, long long g_left_pstride, const double* g_right,
-                         long long g_right_pstride, const int* k_index, const double* omega,
-                         const double* eta_device, const int* lead_status, const double* weight, double* grad_onsite,
-                         double* grad_coupling, double* t_out, int* status_out, void* workspace,
-                         size_t workspace_bytes, void* stream) {
+}  // extern "C"
+
+static int fail2(int code, const char* name, const char* what) {
+  char msg[256];
+  std::snprintf(msg, sizeof(msg), "%s: %s", name, what);
+  return fail(code, msg);
+}
+static int cuda_fail2(const char* name, const char* what) {
+  char msg[256];
+  std::snprintf(msg, sizeof(msg), "%s: %s", name, what);
+  return cuda_fail(msg);
+}
+
+// Shared body of negf_rgf_adjoint_f64 and negf_rgf_adjoint_sigma_f64 (which
+// also writes the per-point self-energy adjoints when sig_adj_l/r are set).
+static int rgf_adjoint_common(const char* name, int n_dev, int n_lead_l, int n_lead_r, int n_layers, int batch,
+                              const double* onsite, long long onsite_kstride, long long onsite_lstride,
+                              const double* coupling, long long coupling_kstride, long long coupling_lstride,
+                              const double* v_left, long long v_left_kstride, const double* v_right,
+                              long long v_right_kstride, const double* g_left, long long g_left_pstride,
+                              const double* g_right, long long g_right_pstride, const int* k_index,
+                              const double* omega, const double* eta_device, const int* lead_status,
+                              const double* weight, double* grad_onsite, double* grad_coupling, double* t_out,
+                              int* status_out, void* workspace, size_t workspace_bytes, void* stream,
+                              double* sig_adj_l, double* sig_adj_r) {
   if (n_dev <= 0 || n_lead_l <= 0 || n_lead_r <= 0 || n_layers <= 0 || batch < 0)
-    return fail(NEGF_EINVAL, "negf_rgf_adjoint_f64: sizes must be positive");
+    return fail2(NEGF_EINVAL, name, "sizes must be positive");
   if (!onsite || !v_left || !v_right || !g_left || !g_right || !omega || !eta_device || !t_out || !weight ||
       !grad_onsite || (n_layers > 1 && (!coupling || !grad_coupling)))
-    return fail(NEGF_EINVAL, "negf_rgf_adjoint_f64: null pointer");
+    return fail2(NEGF_EINVAL, name, "null pointer");
   if (onsite_kstride < 0 || onsite_lstride < 0 || coupling_kstride < 0 || coupling_lstride < 0 ||
       v_left_kstride < 0 || v_right_kstride < 0 || g_left_pstride < 0 || g_right_pstride < 0)
-    return fail(NEGF_EINVAL, "negf_rgf_adjoint_f64: negative stride");
+    return fail2(NEGF_EINVAL, name, "negative stride");
   const int nmax = max3(n_dev, n_lead_l, n_lead_r);
-  if (nmax > 256) return fail(NEGF_EUNSUPPORTED, "negf_rgf_adjoint_f64: block order above 256");
+  if (nmax > 256) return fail2(NEGF_EUNSUPPORTED, name, "block order above 256");
   const int np = (nmax + 15) / 16 * 16;
   const int grid = negf::grad_grid(np);
-  if (grid <= 0) return cuda_fail("negf_rgf_adjoint_f64: occupancy query");
+  if (grid <= 0) return cuda_fail2(name, "occupancy query");
   if (!workspace || workspace_bytes < kCounterBytes + negf::grad_ws_bytes(np, n_dev, n_layers, grid))
-    return fail(NEGF_EINVAL, "negf_rgf_adjoint_f64: workspace missing or too small");
+    return fail2(NEGF_EINVAL, name, "workspace missing or too small");
   if (batch == 0) return 0;
   negf::GradArgs ga;
   negf::RgfArgs& a = ga.r;
@@ -436,12 +524,112 @@ int negf_rgf_adjoint_f64(int n_dev, int n_lead_l, int n_lead_r, int n_layers, in
   ga.weight = weight;
   ga.grad_d = reinterpret_cast<double2*>(grad_onsite);
   ga.grad_c = reinterpret_cast<double2*>(grad_coupling ? grad_coupling : grad_onsite);
+  ga.sig_adj_l = reinterpret_cast<double2*>(sig_adj_l);
+  ga.sig_adj_r = reinterpret_cast<double2*>(sig_adj_r);
   cudaStream_t st = as_stream(stream);
   if (cudaMemsetAsync(workspace, 0, sizeof(unsigned int), st) != cudaSuccess)
-    return cuda_fail("negf_rgf_adjoint_f64: counter reset");
+    return cuda_fail2(name, "counter reset");
   const int rc = negf::grad_f64_launch(ga, np, grid,
                                        reinterpret_cast<double2*>(static_cast<char*>(workspace) + kCounterBytes), st);
-  if (rc != 0) return cuda_fail("negf_rgf_adjoint_f64");
+  if (rc != 0) return cuda_fail2(name, "launch");
+  return 0;
+}
+
+extern "C" {
+
+int negf_rgf_adjoint_f64(int n_dev, int n_lead_l, int n_lead_r, int n_layers, int batch, const double* onsite,
+                         long long onsite_kstride, long long onsite_lstride, const double* coupling,
+                         long long coupling_kstride, long long coupling_lstride, const double* v_left,
+                         long long v_left_kstride, const double* v_right, long long v_right_kstride,
+                         const double* g_left, long long g_left_pstride, const double* g_right,
+                         long long g_right_pstride, const int* k_index, const double* omega,
+                         const double* eta_device, const int* lead_status, const double* weight, double* grad_onsite,
+                         double* grad_coupling, double* t_out, int* status_out, void* workspace,
+                         size_t workspace_bytes, void* stream) {
+  return rgf_adjoint_common("negf_rgf_adjoint_f64", n_dev, n_lead_l, n_lead_r, n_layers, batch, onsite,
+                            onsite_kstride, onsite_lstride, coupling, coupling_kstride, coupling_lstride, v_left,
+                            v_left_kstride, v_right, v_right_kstride, g_left, g_left_pstride, g_right,
+                            g_right_pstride, k_index, omega, eta_device, lead_status, weight, grad_onsite,
+                            grad_coupling, t_out, status_out, workspace, workspace_bytes, stream, nullptr, nullptr);
+}
+
+int negf_rgf_adjoint_sigma_f64(int n_dev, int n_lead_l, int n_lead_r, int n_layers, int batch, const double* onsite,
+                               long long onsite_kstride, long long onsite_lstride, const double* coupling,
+                               long long coupling_kstride, long long coupling_lstride, const double* v_left,
+                               long long v_left_kstride, const double* v_right, long long v_right_kstride,
+                               const double* g_left, long long g_left_pstride, const double* g_right,
+                               long long g_right_pstride, const int* k_index, const double* omega,
+                               const double* eta_device, const int* lead_status, const double* weight,
+                               double* grad_onsite, double* grad_coupling, double* sigma_adj_left,
+                               double* sigma_adj_right, double* t_out, int* status_out, void* workspace,
+                               size_t workspace_bytes, void* stream) {
+  if (!sigma_adj_left && !sigma_adj_right)
+    return fail(NEGF_EINVAL, "negf_rgf_adjoint_sigma_f64: no self-energy adjoint output");
+  return rgf_adjoint_common("negf_rgf_adjoint_sigma_f64", n_dev, n_lead_l, n_lead_r, n_layers, batch, onsite,
+                            onsite_kstride, onsite_lstride, coupling, coupling_kstride, coupling_lstride, v_left,
+                            v_left_kstride, v_right, v_right_kstride, g_left, g_left_pstride, g_right,
+                            g_right_pstride, k_index, omega, eta_device, lead_status, weight, grad_onsite,
+                            grad_coupling, t_out, status_out, workspace, workspace_bytes, stream, sigma_adj_left,
+                            sigma_adj_right);
+}
+
+size_t negf_sgf_adjoint_workspace_bytes(int n_lead, int n_dev) {
+  if (n_lead <= 0 || n_dev <= 0 || n_lead > 256 || n_dev > 256) return 0;
+  const int np = (max3(n_lead, n_dev, 1) + 15) / 16 * 16;
+  const int grid = negf::sgf_adj_grid(np);
+  if (grid <= 0) return 0;
+  return kCounterBytes + negf::sgf_adj_ws_bytes(np, grid);
+}
+
+int negf_sgf_adjoint_f64(int n_lead, int n_dev, int batch, const double* h01, const double* h10,
+                         long long lead_stride, const double* v, long long v_kstride, const double* g,
+                         long long g_pstride, const double* sigma_adj, const int* k_index, const int* lead_status,
+                         double tol, int maxiter, double* grad_h00, double* grad_h01, double* grad_h10,
+                         double* grad_v, int* iters_out, int* status_out, void* workspace, size_t workspace_bytes,
+                         void* stream) {
+  if (n_lead <= 0 || n_dev <= 0 || batch < 0)
+    return fail(NEGF_EINVAL, "negf_sgf_adjoint_f64: sizes must be positive");
+  if (!h01 || !v || !g || !sigma_adj || !grad_h00 || !grad_h01 || !grad_v || (h10 && !grad_h10))
+    return fail(NEGF_EINVAL, "negf_sgf_adjoint_f64: null pointer");
+  if (lead_stride < 0 || v_kstride < 0 || g_pstride < 0)
+    return fail(NEGF_EINVAL, "negf_sgf_adjoint_f64: negative stride");
+  if (maxiter <= 0 || !(tol > 0.0)) return fail(NEGF_EINVAL, "negf_sgf_adjoint_f64: maxiter and tol must be positive");
+  if (n_lead > 256 || n_dev > 256) return fail(NEGF_EUNSUPPORTED, "negf_sgf_adjoint_f64: block order above 256");
+  const int np = (max3(n_lead, n_dev, 1) + 15) / 16 * 16;
+  const int grid = negf::sgf_adj_grid(np);
+  if (grid <= 0) return cuda_fail("negf_sgf_adjoint_f64: occupancy query");
+  if (!workspace || workspace_bytes < kCounterBytes + negf::sgf_adj_ws_bytes(np, grid))
+    return fail(NEGF_EINVAL, "negf_sgf_adjoint_f64: workspace missing or too small");
+  if (batch == 0) return 0;
+  negf::SgfAdjArgs sa;
+  sa.nl = n_lead;
+  sa.n = n_dev;
+  sa.batch = batch;
+  sa.h01 = reinterpret_cast<const double2*>(h01);
+  sa.h10 = reinterpret_cast<const double2*>(h10);
+  sa.lead_stride = lead_stride;
+  sa.V = reinterpret_cast<const double2*>(v);
+  sa.v_ks = v_kstride;
+  sa.g = reinterpret_cast<const double2*>(g);
+  sa.g_ps = g_pstride;
+  sa.xs = reinterpret_cast<const double2*>(sigma_adj);
+  sa.kidx = k_index;
+  sa.lead_status = lead_status;
+  sa.tol = tol;
+  sa.maxiter = maxiter;
+  sa.grad_h00 = reinterpret_cast<double2*>(grad_h00);
+  sa.grad_h01 = reinterpret_cast<double2*>(grad_h01);
+  sa.grad_h10 = h10 ? reinterpret_cast<double2*>(grad_h10) : nullptr;
+  sa.grad_v = reinterpret_cast<double2*>(grad_v);
+  sa.iters_out = iters_out;
+  sa.status_out = status_out;
+  sa.counter = reinterpret_cast<unsigned*>(workspace);
+  cudaStream_t st = as_stream(stream);
+  if (cudaMemsetAsync(workspace, 0, sizeof(unsigned), st) != cudaSuccess)
+    return cuda_fail("negf_sgf_adjoint_f64: counter reset");
+  if (negf::sgf_adj_launch(sa, np, grid, reinterpret_cast<double2*>(static_cast<char*>(workspace) + kCounterBytes),
+                           st) != 0)
+    return cuda_fail("negf_sgf_adjoint_f64");
   return 0;
 }
 

@@ -51,6 +51,33 @@ struct GradArgs {
   const double* weight;  // [batch] dKappa/dT of each point
   double2* grad_d;       // [K][L][n][n]    += weight X_ii
   double2* grad_c;       // [K][L-1][n][n]  += weight (X_{i+1,i} + X_{i,i+1}^H)
+  double2* sig_adj_l;    // [batch][n][n] or nullptr: weight dT/dSigma_L (X_00 + i G Gamma_R G^H)
+  double2* sig_adj_r;    // [batch][n][n] or nullptr: weight dT/dSigma_R (X_{L-1,L-1} + i G^H Gamma_L G)
+};
+
+// Adjoint of the surface GF fixed point g = (z - H00 - H01 g H10)^-1 and of
+// Sigma = V g V^H, per point, accumulated per lead set k.
+struct SgfAdjArgs {
+  int nl, n, batch;        // lead order, device order
+  const double2* h01;
+  const double2* h10;      // nullptr: H10 = H01^H (its gradient is folded into grad_h01)
+  long long lead_stride;   // complex elements between lead sets
+  const double2* V;        // [.][n][nl] device-to-lead coupling of this lead
+  long long v_ks;
+  const double2* g;        // [batch][nl][nl] surface GFs
+  long long g_ps;
+  const double2* xs;       // [batch][n][n] weighted dT/dSigma (convention dT = 2 Re Tr[dSigma X])
+  const int* kidx;
+  const int* lead_status;  // nonzero: skip the point
+  double tol;
+  int maxiter;
+  double2* grad_h00;       // [K][nl][nl] += X-convention adjoints
+  double2* grad_h01;
+  double2* grad_h10;       // nullptr when h10 is nullptr
+  double2* grad_v;         // [K|1][nl][n]
+  int* iters_out;
+  int* status_out;
+  unsigned* counter;
 };
 
 // Full device Green's function: RgfArgs plus the outputs.
@@ -85,6 +112,12 @@ int rgf_mixed_grid(int np);
 size_t rgf_mixed_ws_bytes(int np, int n, int grid);
 int rgf_mixed_launch(const RgfArgs& a, int np, int grid, void* ws, cudaStream_t st);
 
+// Refined device solve (FP32 factors, FP64 iterative refinement), orders 1..256.
+int rgf_refine_grid(int np);
+size_t rgf_refine_ws_bytes(int np, int n, int L, int grid);
+int rgf_refine_launch(const RgfArgs& a, int np, int grid, void* ws, double tol, int maxit, int* steps_out,
+                      cudaStream_t st);
+
 // Uneven batch (negf_batch.cu).
 int batch_max_grid(int npmax, int mixed, int minb);
 size_t batch_ws_bytes(int npmax, int grid);
@@ -99,6 +132,10 @@ int full_f64_launch(const FullArgs& fa, int np, int grid, double2* ws, cudaStrea
 size_t grad_ws_bytes(int np, int n, int L, int grid);
 int grad_grid(int np);
 int grad_f64_launch(const GradArgs& ga, int np, int grid, double2* ws, cudaStream_t st);
+
+size_t sgf_adj_ws_bytes(int np, int grid);
+int sgf_adj_grid(int np);
+int sgf_adj_launch(const SgfAdjArgs& sa, int np, int grid, double2* ws, cudaStream_t st);
 
 int heat_current_launch(const double* om, const double* t, int W, int n_spectra, double temp_l, double temp_r,
                         double* out, cudaStream_t st);

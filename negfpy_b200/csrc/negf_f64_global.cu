@@ -337,6 +337,18 @@ __global__ void __launch_bounds__(kThreads, 2) rgf_grad_f64_kernel(GradArgs ga, 
         }
       }
     }
+    // Contact terms of dT/dSigma: Sigma_L enters A_00 (like D_00) and Gamma_L,
+    // so dT/dSigma_L = X_00 + i G Gamma_R G^H; likewise dT/dSigma_R =
+    // X_{L-1,L-1} + i G^H Gamma_L G, with G = G_{0,L-1} (slot 0 of gl).
+    const bool want_l = ga.sig_adj_l != nullptr, want_r = ga.sig_adj_r != nullptr;
+    if (status == kOk && want_l) {
+      gemm_to<false, false>(W, gl, GR, NP, kch);
+      gemm_to<false, true>(Mb, W, gl, NP, kch);
+    }
+    if (status == kOk && want_r) {
+      gemm_to<true, false>(W, gl, GL, NP, kch);
+      gemm_to<false, false>(Xs, W, gl, NP, kch);
+    }
     // 4. first block row and the adjoint blocks
     for (int i = 0; i < L && status == kOk; ++i) {
       gemm_to<false, false>(Ac, gl + i * M2, Y, NP, kch);
@@ -346,6 +358,14 @@ __global__ void __launch_bounds__(kThreads, 2) rgf_grad_f64_kernel(GradArgs ga, 
         if (r < n && c < n) {
           const double2 v = Xa[e];
           atomic_cadd(gdk + (long long)i * n * n + r * n + c, make_double2(wgt * v.x, wgt * v.y));
+          if (i == 0 && want_l) {
+            const double2 zt = Mb[e];
+            ga.sig_adj_l[(long long)p * n * n + r * n + c] = make_double2(wgt * (v.x - zt.y), wgt * (v.y + zt.x));
+          }
+          if (i == L - 1 && want_r) {
+            const double2 zt = Xs[e];
+            ga.sig_adj_r[(long long)p * n * n + r * n + c] = make_double2(wgt * (v.x - zt.y), wgt * (v.y + zt.x));
+          }
         }
       }
       __syncthreads();  // Xa is rewritten next
@@ -376,6 +396,163 @@ __global__ void __launch_bounds__(kThreads, 2) rgf_grad_f64_kernel(GradArgs ga, 
     if (tid == 0) {
       a.T_out[p] = (status == kOk) ? tval : __longlong_as_double(0x7ff8000000000000ULL);
       if (a.status_out) a.status_out[p] = status;
+    }
+    __syncthreads();
+  }
+}
+
+// ------------------------------------------------ adjoint of the surface GF --
+// dst += op(A) op(B) (each thread updates only the elements of its own tiles).
+template <bool AC, bool BC>
+__device__ void gemm_add(double2* dst, const double2* A, const double2* B, int NP, int kch) {
+  const int warp = threadIdx.x >> 5, np16 = NP >> 4, nt = np16 * np16;
+  for (int tt = warp; tt < nt; tt += kWarps) {
+    const Tile T = tile_of(tt, np16);
+    Acc c;
+    tile_mm<AC, BC>(c, A, NP, B, NP, kch, T);
+#pragma unroll
+    for (int j = 0; j < 2; ++j)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        double2* d = dst + (long long)tr(T, q) * NP + tc(T, j, q);
+        *d = cadd(*d, c.get(j, q));
+      }
+  }
+  __syncthreads();
+}
+
+// Per point, with the surface GF g of the lead (negfpy core/surface_gf.py:18-81
+// computes it by decimation) and the weighted adjoint X of Sigma = V g V^H
+// from rgf_grad_f64_kernel (dT = 2 Re Tr[dSigma X]):
+//
+//   gbar = V^H X V,   Vbar = g V^H X + g^H V^H X^H            (dT = 2 Re Tr[dV Vbar])
+//
+// g solves g = (z - H00 - H01 g H10)^-1, so with P = g H01 and Q = H10 g,
+//   dg - P dg Q = g (dH00 + dH01 g H10 + H01 g dH10) g,
+// and Tr[dg gbar] = Tr[(dH00 + dH01 g H10 + H01 g dH10) g Lam g] where Lam
+// solves the transposed equation Lam - Q Lam P = gbar.  Lam = sum_k Q^k gbar P^k
+// is summed by doubling (Smith's method): Lam += A Lam B, A <- A^2, B <- B^2
+// from A = Q, B = P, until max(max|A|, max|B|) < tol; no inverse is needed and
+// nothing is differentiated through the decimation sweeps.  Then
+//   H00bar = g Lam g,  H01bar = g H10 H00bar,  H10bar = H00bar P,
+// added into the per-k accumulators (with H10 = H01^H, H10bar^H is added to
+// H01bar instead).  Status: kMaxIter if the doubling does not converge within
+// maxiter, kNonFinite on inf/nan.
+__global__ void __launch_bounds__(kThreads, 2) sgf_adjoint_f64_kernel(SgfAdjArgs sa, int NP, double2* ws) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  double* red = reinterpret_cast<double*>(smraw + ((gjs_bytes(NP) + 15) / 16) * 16);
+  __shared__ int s_point;
+  const int nl = sa.nl, n = sa.n, tid = threadIdx.x;
+  const int kl = (nl + 7) >> 3, kd = (n + 7) >> 3;
+  const long long M2 = (long long)NP * NP;
+  double2* base = ws + (long long)blockIdx.x * 15 * M2;
+  double2 *Vb = base, *Xb = base + M2, *Gb = base + 2 * M2, *T1 = base + 3 * M2, *T2 = base + 4 * M2;
+  double2 *Gbar = base + 5 * M2, *Pk = base + 6 * M2, *Aq = base + 7 * M2, *Bp = base + 8 * M2;
+  double2 *Aq2 = base + 9 * M2, *Bp2 = base + 10 * M2, *Lam = base + 11 * M2, *Tt = base + 12 * M2;
+  double2 *H01b = base + 13 * M2, *H10b = base + 14 * M2;
+
+  for (;;) {
+    if (tid == 0) s_point = (int)atomicAdd(sa.counter, 1u);
+    __syncthreads();
+    const int p = s_point;
+    __syncthreads();
+    if (p >= sa.batch) break;
+    const int lst = sa.lead_status ? sa.lead_status[p] : 0;
+    if (lst != kOk) {
+      if (tid == 0) {
+        if (sa.status_out) sa.status_out[p] = lst;
+        if (sa.iters_out) sa.iters_out[p] = 0;
+      }
+      continue;
+    }
+    const long long k = sa.kidx ? (long long)sa.kidx[p] : 0;
+    const double2* h01 = sa.h01 + k * sa.lead_stride;
+    const double2* h10 = sa.h10 ? sa.h10 + k * sa.lead_stride : nullptr;
+    load_pad(Vb, sa.V + k * sa.v_ks, n, nl, NP, 0.0);
+    load_pad(Xb, sa.xs + (long long)p * n * n, n, n, NP, 0.0);
+    load_pad(Gb, sa.g + (long long)p * sa.g_ps, nl, nl, NP, 0.0);
+    load_pad(H01b, h01, nl, nl, NP, 0.0);
+    if (h10) load_pad(H10b, h10, nl, nl, NP, 0.0);
+    __syncthreads();
+    // gbar and Vbar
+    gemm_to<false, false>(T1, Xb, Vb, NP, kd);     // X V          (n x nl)
+    gemm_to<true, false>(Gbar, Vb, T1, NP, kd);    // V^H X V      (nl x nl)
+    gemm_to<true, false>(T2, Vb, Xb, NP, kd);      // V^H X        (nl x n)
+    gemm_to<false, false>(Aq, Gb, T2, NP, kl);     // g V^H X      (nl x n)
+    gemm_to<false, false>(Bp, T1, Gb, NP, kl);     // X V g        (n x nl)
+    {
+      double2* gv = sa.grad_v + k * (sa.v_ks ? (long long)nl * n : 0);
+      for (long long e = tid; e < M2; e += kThreads) {
+        const int r = (int)(e / NP), c = (int)(e - (long long)r * NP);
+        if (r < nl && c < n) atomic_cadd(gv + (long long)r * n + c, cadd(Aq[e], cconj(Bp[(long long)c * NP + r])));
+      }
+      __syncthreads();  // Aq and Bp are rewritten next
+    }
+    // P = g H01, Q = H10 g
+    gemm_to<false, false>(Pk, Gb, H01b, NP, kl);
+    if (h10) gemm_to<false, false>(Aq, H10b, Gb, NP, kl);
+    else gemm_to<true, false>(Aq, H01b, Gb, NP, kl);
+    copy_mat(Bp, Pk, NP);
+    copy_mat(Lam, Gbar, NP);
+    // Smith doubling for Lam - Q Lam P = gbar
+    int status = kOk, it = 0;
+    for (;;) {
+      ++it;
+      gemm_to<false, false>(Tt, Aq, Lam, NP, kl);
+      gemm_add<false, false>(Lam, Tt, Bp, NP, kl);
+      gemm_to<false, false>(Aq2, Aq, Aq, NP, kl);
+      gemm_to<false, false>(Bp2, Bp, Bp, NP, kl);
+      double2* t = Aq;
+      Aq = Aq2;
+      Aq2 = t;
+      t = Bp;
+      Bp = Bp2;
+      Bp2 = t;
+      double m = 0.0;
+      int bad = 0;
+      for (long long e = tid; e < M2; e += kThreads) {
+        const double2 a = Aq[e], b = Bp[e], l = Lam[e];
+        bad |= !(cfinite(a) && cfinite(b) && cfinite(l));
+        m = fmax(m, fmax(fmax(fabs(a.x), fabs(a.y)), fmax(fabs(b.x), fabs(b.y))));
+      }
+      if (block_any(bad)) {
+        status = kNonFinite;
+        break;
+      }
+      m = block_max(m, red);
+      if (m < sa.tol) break;
+      if (it >= sa.maxiter) {
+        status = kMaxIter;
+        break;
+      }
+    }
+    if (status == kOk) {
+      gemm_to<false, false>(Tt, Lam, Gb, NP, kl);    // Lam g
+      gemm_to<false, false>(T1, Gb, Tt, NP, kl);     // H00bar = g Lam g
+      if (h10) gemm_to<false, false>(Tt, Gb, H10b, NP, kl);   // g H10
+      else gemm_to<false, true>(Tt, Gb, H01b, NP, kl);
+      gemm_to<false, false>(T2, Tt, T1, NP, kl);     // H01bar = g H10 H00bar
+      gemm_to<false, false>(Tt, T1, Pk, NP, kl);     // H10bar = H00bar P
+      double2* g00 = sa.grad_h00 + k * (long long)nl * nl;
+      double2* g01 = sa.grad_h01 + k * (long long)nl * nl;
+      double2* g10 = sa.grad_h10 ? sa.grad_h10 + k * (long long)nl * nl : nullptr;
+      for (long long e = tid; e < M2; e += kThreads) {
+        const int r = (int)(e / NP), c = (int)(e - (long long)r * NP);
+        if (r < nl && c < nl) {
+          atomic_cadd(g00 + r * nl + c, T1[e]);
+          if (h10) {
+            atomic_cadd(g01 + r * nl + c, T2[e]);
+            if (g10) atomic_cadd(g10 + r * nl + c, Tt[e]);
+          } else {
+            atomic_cadd(g01 + r * nl + c, cadd(T2[e], cconj(Tt[(long long)c * NP + r])));
+          }
+        }
+      }
+    }
+    __syncthreads();
+    if (tid == 0) {
+      if (sa.status_out) sa.status_out[p] = status;
+      if (sa.iters_out) sa.iters_out[p] = it;
     }
     __syncthreads();
   }
@@ -548,6 +725,19 @@ int full_grid(int np) {
 int full_f64_launch(const FullArgs& fa, int np, int grid, double2* ws, cudaStream_t st) {
   if (fa.r.batch <= 0) return 0;
   glob::rgf_full_f64_kernel<<<grid, glob::kThreads, glob::smem_bytes(np), st>>>(fa, np, ws);
+  return cudaGetLastError() == cudaSuccess ? 0 : -3;
+}
+size_t sgf_adj_ws_bytes(int np, int grid) { return (size_t)grid * 15 * (size_t)np * np * 16; }
+int sgf_adj_grid(int np) {
+  const int g = glob::occupancy_grid(glob::sgf_adjoint_f64_kernel, np);
+  int dev = 0, nsm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  return g > 2 * nsm ? 2 * nsm : g;
+}
+int sgf_adj_launch(const SgfAdjArgs& sa, int np, int grid, double2* ws, cudaStream_t st) {
+  if (sa.batch <= 0) return 0;
+  glob::sgf_adjoint_f64_kernel<<<grid, glob::kThreads, glob::smem_bytes(np), st>>>(sa, np, ws);
   return cudaGetLastError() == cudaSuccess ? 0 : -3;
 }
 int grad_f64_launch(const GradArgs& ga, int np, int grid, double2* ws, cudaStream_t st) {

@@ -86,11 +86,12 @@ struct Acc32 {
 };
 
 // acc = op(A) op(B) for one 16 x 16 tile (FP32 matrices, row stride ld),
-// contraction over kch chunks of 8; AC / BC: conjugate-transposed operand.
-template <bool AC, bool BC>
+// contraction over kch chunks of 8 (ADD: acc += op(A) op(B)); AC / BC:
+// conjugate-transposed operand.
+template <bool AC, bool BC, bool ADD = false>
 __device__ __forceinline__ void tile_mm32(Acc32& c, const float2* __restrict__ A, const float2* __restrict__ B, int ld,
                                           int kch, const Tile& T) {
-  c.zero();
+  if (!ADD) c.zero();
   for (int kc = 0; kc < kch; ++kc) {
     const int k0 = kc * 8;
     AFrag a;

@@ -57,13 +57,13 @@ __device__ __forceinline__ Tile tile_of(int tt, int np16) {
 __device__ __forceinline__ int tr(const Tile& T, int q) { return T.m0 + T.g + 8 * (q >> 1); }
 __device__ __forceinline__ int tc(const Tile& T, int j, int q) { return T.n0 + 8 * j + 2 * T.t + (q & 1); }
 
-// acc = op(A) op(B) for one 16 x 16 tile, contraction over kch chunks of 8.
-// AC / BC: operand is the conjugate transpose of the stored matrix.
-// lda / ldb: row strides of the stored matrices.
-template <bool AC, bool BC>
+// acc = op(A) op(B) for one 16 x 16 tile, contraction over kch chunks of 8
+// (ADD: acc += op(A) op(B)).  AC / BC: operand is the conjugate transpose of
+// the stored matrix.  lda / ldb: row strides of the stored matrices.
+template <bool AC, bool BC, bool ADD = false>
 __device__ __forceinline__ void tile_mm(Acc& c, const double2* __restrict__ A, int lda, const double2* __restrict__ B,
                                         int ldb, int kch, const Tile& T) {
-  c.zero();
+  if (!ADD) c.zero();
   for (int kc = 0; kc < kch; ++kc) {
     const int k0 = kc * 8;
     double ar[4], ai[4];

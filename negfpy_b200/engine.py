@@ -131,11 +131,86 @@ def rgf_transmission(onsite: torch.Tensor, coupling: torch.Tensor | None, n_laye
     return T, st
 
 
+REFINE_TOL = 1e-12
+REFINE_MAX_STEPS = 4
+
+
+def rgf_transmission_refine64(onsite, coupling, n_layers, vl, vr, gl, gr, omega, eta_dev, k_index, lead_status,
+                              stream=None, tol: float = REFINE_TOL, max_steps: int = REFINE_MAX_STEPS):
+    """T, status and refinement steps for P points from FP32 factors refined
+    to FP64 accuracy (``negf_rgf_transmission_refined``); blocks as in
+    ``rgf_transmission``.  Points that do not converge report
+    ``_lib.REFINE_FAIL`` (no fallback here)."""
+    lib = _lib.load()
+    dev = _dev()
+    K, Lo, n, _ = onsite.shape
+    nl, nr = int(vl.shape[-1]), int(vr.shape[-1])
+    P = int(omega.shape[0])
+    T = torch.empty(P, dtype=RDT, device=dev)
+    st = torch.empty(P, dtype=torch.int32, device=dev)
+    steps = torch.zeros(P, dtype=torch.int32, device=dev)
+    if P == 0:
+        return T, st, steps
+    on_ks = Lo * n * n if K > 1 else 0
+    on_ls = 0 if Lo == 1 else n * n
+    if coupling is None or n_layers == 1:
+        cp, cp_ks, cp_ls = None, 0, 0
+    else:
+        Kc, Lc = coupling.shape[0], coupling.shape[1]
+        cp, cp_ks, cp_ls = coupling, (Lc * n * n if Kc > 1 else 0), (0 if Lc == 1 else n * n)
+    need = int(lib.negf_rgf_refined_workspace_bytes(n, nl, nr, int(n_layers)))
+    if need == 0:
+        raise RuntimeError(f"block order {max(n, nl, nr)} is not supported by the refined kernel")
+    ws = _workspace(need, dev, "rgf_refined")
+    if k_index is not None:
+        k_index = k_index.to(device=dev, dtype=torch.int32).contiguous()
+    rc = lib.negf_rgf_transmission_refined(
+        n, nl, nr, int(n_layers), P, _lib.ptr(onsite), on_ks, on_ls, _lib.ptr(cp), cp_ks, cp_ls, _lib.ptr(vl),
+        n * nl if vl.shape[0] > 1 else 0, _lib.ptr(vr), n * nr if vr.shape[0] > 1 else 0, _lib.ptr(gl), nl * nl,
+        _lib.ptr(gr), nr * nr, _lib.ptr(k_index), _lib.ptr(omega), _lib.ptr(eta_dev), _lib.ptr(lead_status),
+        float(tol), int(max_steps), _lib.ptr(T), _lib.ptr(st), _lib.ptr(steps), _lib.ptr(ws), ws.numel(),
+        _lib.stream_handle(stream))
+    _lib.check(rc, "negf_rgf_transmission_refined")
+    return T, st, steps
+
+
+def _fallback_f64(T, st, onsite, coupling, n_layers, vl, vr, gl, gr, omega, eta_dev, k_index, lead_status, stream):
+    """Re-solve in FP64 the points whose reduced-precision solve failed while
+    their leads succeeded; returns the number re-solved."""
+    bad = st != 0
+    if lead_status is not None:
+        bad &= lead_status == 0
+    idx = torch.nonzero(bad).flatten()
+    nbad = int(idx.numel())
+    if nbad:
+        ki = None if k_index is None else k_index[idx]
+        t2, s2 = rgf_transmission(onsite, coupling, n_layers, vl, vr, gl[idx].contiguous(), gr[idx].contiguous(),
+                                  omega[idx].contiguous(), eta_dev[idx].contiguous(), ki, None, stream)
+        T[idx] = t2
+        st[idx] = s2
+    return nbad
+
+
 def rgf_transmission_refined(onsite, coupling, n_layers, vl, vr, gl, gr, omega, eta_dev, k_index, lead_status,
-                             stream=None) -> tuple[torch.Tensor, torch.Tensor, int]:
-    """Mixed-precision device solve with an FP64 fallback: points whose FP32
-    sweep failed (singular or non-finite pivot) while their leads succeeded are
-    solved again by the FP64 kernel.  Returns (T, status, number re-solved)."""
+                             stream=None, tol: float = REFINE_TOL, max_steps: int = REFINE_MAX_STEPS):
+    """Refined device solve with an FP64 fallback: FP32 factors and FP64
+    iterative refinement (``rgf_transmission_refine64``); the points that
+    report NEGF_REFINE_FAIL, or a singular / non-finite FP32 pivot, while
+    their leads succeeded are solved again by the FP64 kernel.  Returns
+    (T, status, number re-solved, refinement steps per point)."""
+    T, st, steps = rgf_transmission_refine64(onsite, coupling, n_layers, vl, vr, gl, gr, omega, eta_dev, k_index,
+                                             lead_status, stream, tol, max_steps)
+    nbad = _fallback_f64(T, st, onsite, coupling, n_layers, vl, vr, gl, gr, omega, eta_dev, k_index, lead_status,
+                         stream)
+    return T, st, nbad, steps
+
+
+def rgf_transmission_mixed(onsite, coupling, n_layers, vl, vr, gl, gr, omega, eta_dev, k_index, lead_status,
+                           stream=None) -> tuple[torch.Tensor, torch.Tensor, int]:
+    """Mixed-precision device solve (FP32 sweep, no refinement) with an FP64
+    fallback: points whose FP32 sweep failed (singular or non-finite pivot)
+    while their leads succeeded are solved again by the FP64 kernel.  Returns
+    (T, status, number re-solved)."""
     T, st = rgf_transmission(onsite, coupling, n_layers, vl, vr, gl, gr, omega, eta_dev, k_index, lead_status,
                              stream, precision="mixed")
     bad = st != 0
@@ -194,13 +269,16 @@ def device_green(onsite: torch.Tensor, coupling: torch.Tensor | None, n_layers: 
 def rgf_adjoint(onsite: torch.Tensor, coupling: torch.Tensor, n_layers: int, vl: torch.Tensor, vr: torch.Tensor,
                 gl: torch.Tensor, gr: torch.Tensor, omega: torch.Tensor, eta_dev: torch.Tensor,
                 k_index: torch.Tensor, lead_status: torch.Tensor | None, weight: torch.Tensor,
-                stream=None) -> tuple[torch.Tensor, torch.Tensor, torch.Tensor, torch.Tensor]:
+                stream=None, want_sigma: bool = False):
     """Vector-Jacobian product of T with respect to the device blocks.
 
     Layer-resolved blocks ``onsite`` ``[K, L, n, n]`` and ``coupling`` ``[K, L-1, n, n]``
     (no stride-0 sharing: every block is a variable).  Returns (T, status,
     grad_onsite, grad_coupling) with sum_p weight[p] dT_p = 2 Re sum Tr[dD X]
-    over the returned adjoint blocks (``negf_rgf_adjoint_f64``)."""
+    over the returned adjoint blocks (``negf_rgf_adjoint_f64``).  With
+    ``want_sigma`` it also returns the per-point weighted adjoints of the two
+    contact self-energies ``[P, n, n]`` (``negf_rgf_adjoint_sigma_f64``), the
+    input of ``sgf_adjoint``."""
     lib = _lib.load()
     dev = _dev()
     K, L, n, _ = onsite.shape
@@ -212,8 +290,10 @@ def rgf_adjoint(onsite: torch.Tensor, coupling: torch.Tensor, n_layers: int, vl:
     st = torch.empty(P, dtype=torch.int32, device=dev)
     g_on = torch.zeros((K, L, n, n), dtype=CDT, device=dev)
     g_cp = torch.zeros((K, max(L - 1, 1), n, n), dtype=CDT, device=dev)
+    xs_l = torch.zeros((P, n, n), dtype=CDT, device=dev) if want_sigma else None
+    xs_r = torch.zeros((P, n, n), dtype=CDT, device=dev) if want_sigma else None
     if P == 0:
-        return T, st, g_on, g_cp
+        return (T, st, g_on, g_cp, xs_l, xs_r) if want_sigma else (T, st, g_on, g_cp)
     if L > 1 and (coupling is None or tuple(coupling.shape) != (K, L - 1, n, n)):
         raise ValueError("rgf_adjoint needs coupling blocks [K, L-1, n, n]")
     need = int(lib.negf_adjoint_workspace_bytes(n, nl, nr, L))
@@ -224,14 +304,64 @@ def rgf_adjoint(onsite: torch.Tensor, coupling: torch.Tensor, n_layers: int, vl:
     vl_ks = n * nl if vl.shape[0] > 1 else 0
     vr_ks = n * nr if vr.shape[0] > 1 else 0
     cp = coupling if L > 1 else None
-    rc = lib.negf_rgf_adjoint_f64(
-        n, nl, nr, L, P, _lib.ptr(onsite), L * n * n, n * n, _lib.ptr(cp), (L - 1) * n * n, n * n, _lib.ptr(vl),
-        vl_ks, _lib.ptr(vr), vr_ks, _lib.ptr(gl), nl * nl, _lib.ptr(gr), nr * nr, _lib.ptr(k_index),
-        _lib.ptr(omega), _lib.ptr(eta_dev), _lib.ptr(lead_status), _lib.ptr(weight), _lib.ptr(g_on),
-        _lib.ptr(g_cp if L > 1 else None), _lib.ptr(T), _lib.ptr(st), _lib.ptr(ws), ws.numel(),
-        _lib.stream_handle(stream))
+    common = (n, nl, nr, L, P, _lib.ptr(onsite), L * n * n, n * n, _lib.ptr(cp), (L - 1) * n * n, n * n,
+              _lib.ptr(vl), vl_ks, _lib.ptr(vr), vr_ks, _lib.ptr(gl), nl * nl, _lib.ptr(gr), nr * nr,
+              _lib.ptr(k_index), _lib.ptr(omega), _lib.ptr(eta_dev), _lib.ptr(lead_status), _lib.ptr(weight),
+              _lib.ptr(g_on), _lib.ptr(g_cp if L > 1 else None))
+    tail = (_lib.ptr(T), _lib.ptr(st), _lib.ptr(ws), ws.numel(), _lib.stream_handle(stream))
+    if want_sigma:
+        rc = lib.negf_rgf_adjoint_sigma_f64(*common, _lib.ptr(xs_l), _lib.ptr(xs_r), *tail)
+        _lib.check(rc, "negf_rgf_adjoint_sigma_f64")
+        return T, st, g_on, g_cp, xs_l, xs_r
+    rc = lib.negf_rgf_adjoint_f64(*common, *tail)
     _lib.check(rc, "negf_rgf_adjoint_f64")
     return T, st, g_on, g_cp
+
+
+def sgf_adjoint(d01: torch.Tensor, d10: torch.Tensor | None, v: torch.Tensor, g: torch.Tensor,
+                sigma_adj: torch.Tensor, k_index: torch.Tensor | None, lead_status: torch.Tensor | None = None,
+                tol: float = 1e-12, maxiter: int = 200, stream=None) -> dict:
+    """Adjoint of the lead surface GF and of Sigma = V g V^H (``negf_sgf_adjoint_f64``).
+
+    ``d01``/``d10`` ``[K, nl, nl]`` (d10 None: d01^H), ``v`` ``[K|1, n, nl]``,
+    ``g`` ``[P, nl, nl]`` the surface GFs, ``sigma_adj`` ``[P, n, n]`` the
+    weighted self-energy adjoints of ``rgf_adjoint(want_sigma=True)``.
+    Returns the per-k adjoint blocks (dT = 2 Re Tr[dH X]) ``h00``, ``h01``,
+    ``h10`` (None when d10 is None: its part is folded into ``h01``) of shape
+    ``[K, nl, nl]``, ``v`` of shape ``[K|1, nl, n]``, and per-point
+    ``iters``/``status``."""
+    lib = _lib.load()
+    dev = _dev()
+    if d01.dim() == 2:
+        d01 = d01[None]
+        d10 = None if d10 is None else d10[None]
+    K, nl, _ = d01.shape
+    n = int(v.shape[-2])
+    P = int(g.shape[0])
+    gh00 = torch.zeros((K, nl, nl), dtype=CDT, device=dev)
+    gh01 = torch.zeros((K, nl, nl), dtype=CDT, device=dev)
+    gh10 = None if d10 is None else torch.zeros((K, nl, nl), dtype=CDT, device=dev)
+    gv = torch.zeros((v.shape[0], nl, n), dtype=CDT, device=dev)
+    iters = torch.zeros(P, dtype=torch.int32, device=dev)
+    status = torch.zeros(P, dtype=torch.int32, device=dev)
+    out = {"h00": gh00, "h01": gh01, "h10": gh10, "v": gv, "iters": iters, "status": status}
+    if P == 0:
+        return out
+    need = int(lib.negf_sgf_adjoint_workspace_bytes(nl, n))
+    if need == 0:
+        raise RuntimeError(f"block order {max(nl, n)} is not supported by the surface-GF adjoint kernel")
+    ws = _workspace(need, dev, "sgf_adjoint")
+    if k_index is not None:
+        k_index = k_index.to(device=dev, dtype=torch.int32).contiguous()
+    rc = lib.negf_sgf_adjoint_f64(nl, n, P, _lib.ptr(d01.contiguous()), _lib.ptr(None if d10 is None else
+                                                                                d10.contiguous()),
+                                  nl * nl if K > 1 else 0, _lib.ptr(v.contiguous()), n * nl if v.shape[0] > 1 else 0,
+                                  _lib.ptr(g.contiguous()), nl * nl, _lib.ptr(sigma_adj.contiguous()),
+                                  _lib.ptr(k_index), _lib.ptr(lead_status), float(tol), int(maxiter),
+                                  _lib.ptr(gh00), _lib.ptr(gh01), _lib.ptr(gh10), _lib.ptr(gv), _lib.ptr(iters),
+                                  _lib.ptr(status), _lib.ptr(ws), ws.numel(), _lib.stream_handle(stream))
+    _lib.check(rc, "negf_sgf_adjoint_f64")
+    return out
 
 
 def kavg(T_wk: torch.Tensor, stream=None) -> torch.Tensor:
@@ -314,12 +444,21 @@ class StackedSystem:
                      chunk: int = 1 << 15, stream=None, precision: str = "f64") -> dict:
         """T, status and decimation counts for P points (float64/int32 tensors).
 
-        ``precision="refined"``: FP64 surface GFs, mixed-precision device solve
-        with the FP64 fallback of ``rgf_transmission_refined``; the result also
-        carries ``fallback`` (points re-solved in FP64)."""
-        if precision not in ("f64", "refined"):
-            raise ValueError(f"unknown precision {precision!r}; expected 'f64' or 'refined'")
+        ``precision``:
+        - "f64": FP64 throughout;
+        - "refined": FP64 surface GFs, the device solve from FP32 factors
+          refined to FP64 accuracy, FP64 re-solve of the points whose
+          refinement fails (``rgf_transmission_refined``); the result also
+          carries ``fallback`` (points re-solved in FP64) and ``steps``
+          (refinement steps per point);
+        - "mixed": FP64 surface GFs, the FP32 sweep without refinement (about
+          FP32 accuracy), FP64 re-solve of failed points
+          (``rgf_transmission_mixed``)."""
+        if precision not in ("f64", "refined", "mixed"):
+            raise ValueError(f"unknown precision {precision!r}; expected 'f64', 'refined' or 'mixed'")
         n_fallback = 0
+        steps_all = torch.zeros(int(omega.shape[0]), dtype=torch.int32, device=_dev()) \
+            if precision == "refined" else None
         dev = _dev()
         P = int(omega.shape[0])
         omega = _r(omega, dev)
@@ -342,8 +481,13 @@ class StackedSystem:
                 rr = sgf_sr(*self.lead_r, om, et, ki, tol, maxiter, stream=stream)
                 lst = torch.where(rl["status"] != 0, rl["status"], rr["status"])
             if precision == "refined":
-                t, s, nb = rgf_transmission_refined(self.onsite, self.coupling, self.n_layers, self.vl, self.vr,
-                                                    rl["g"], rr["g"], om, ed, ki, lst, stream=stream)
+                t, s, nb, stp = rgf_transmission_refined(self.onsite, self.coupling, self.n_layers, self.vl,
+                                                         self.vr, rl["g"], rr["g"], om, ed, ki, lst, stream=stream)
+                n_fallback += nb
+                steps_all[sl] = stp
+            elif precision == "mixed":
+                t, s, nb = rgf_transmission_mixed(self.onsite, self.coupling, self.n_layers, self.vl, self.vr,
+                                                  rl["g"], rr["g"], om, ed, ki, lst, stream=stream)
                 n_fallback += nb
             else:
                 t, s = rgf_transmission(self.onsite, self.coupling, self.n_layers, self.vl, self.vr, rl["g"],
@@ -352,4 +496,5 @@ class StackedSystem:
             st[sl] = s
             itl[sl] = rl["iters"]
             itr[sl] = rr["iters"]
-        return {"T": T, "status": st, "iters_left": itl, "iters_right": itr, "fallback": n_fallback}
+        return {"T": T, "status": st, "iters_left": itl, "iters_right": itr, "fallback": n_fallback,
+                "steps": steps_all}

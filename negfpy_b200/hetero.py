@@ -20,6 +20,14 @@ blocks are linear in theta:
 in theta and in the device site masses (D = M^-1/2 Phi M^-1/2, the pinning
 pin / m included), so gradients reach both through torch autograd from the
 block gradients that the adjoint kernel provides.
+
+The spring tables of the two materials are parameters too: ``phi_a`` and
+``phi_b`` (one value per (site, neighbour vector) key, ``material_keys``)
+set every A-A or B-B bond of the device (unless theta overrides it), the
+half bonds at the device ends, and the periodic lead crystals, whose blocks
+``lead_blocks_torch`` builds differentiably from them and from the masses of
+device layer 0 (lead A) and layer L-1 (lead B).  Lead and device therefore
+share parameters, and gradients reach them through the surface-GF adjoint.
 """
 
 from __future__ import annotations
@@ -80,10 +88,16 @@ class HeteroModel:
         spr_b = {(s, d): rng.uniform(0.8, 1.6) for s in range(self.n_sites) for d in _half_space_neighbours()}
         spr_i = {(s, d): rng.uniform(0.6, 1.4) for s in range(self.n_sites) for d in _half_space_neighbours()}
         self._spr = (spr_a, spr_b, spr_i)
+        # Material spring tables as parameter vectors, one entry per (site, d).
+        self.material_keys = [(s, d) for s in range(self.n_sites) for d in _half_space_neighbours()]
+        self.key_index = {kd: i for i, kd in enumerate(self.material_keys)}
+        self.phi0_a = np.array([spr_a[kd] for kd in self.material_keys])
+        self.phi0_b = np.array([spr_b[kd] for kd in self.material_keys])
         # Bond instances of the device.  Layers -1 and n_layers stand for the
         # leads: a spring crossing the device boundary contributes only its
         # device-side self term (the rest is the lead coupling).
         la, a, lb, b, cy, ev, k0 = [], [], [], [], [], [], []
+        src, key = [], []  # spring source of each bond: 0 fixed (interface), 1 phi_a, 2 phi_b
         for s in range(self.n_sites):  # lead A (layer -1) -> device layer 0
             if self.site_z[s] >= nz_a:
                 continue
@@ -97,6 +111,7 @@ class HeteroModel:
                 la.append(-1), a.append(s), lb.append(0), b.append(s2), cy.append(c)
                 ev.append(np.asarray(d, float) / np.linalg.norm(d))
                 k0.append(spr_a[(s, d)])
+                src.append(1), key.append(self.key_index[(s, d)])
         for l in range(n_layers):
             for s in range(self.n_sites):
                 if not self.active[l, s]:
@@ -113,17 +128,21 @@ class HeteroModel:
                         la.append(l), a.append(s), lb.append(l2), b.append(s2), cy.append(c)
                         ev.append(np.asarray(d, float) / np.linalg.norm(d))
                         k0.append(spr_b[(s, d)])
+                        src.append(2), key.append(self.key_index[(s, d)])
                         continue
                     if not self.active[l2, s2]:
                         continue
                     ma, mb = l < self.split, l2 < self.split
-                    table = spr_a if (ma and mb) else (spr_b if (not ma and not mb) else spr_i)
+                    which = 1 if (ma and mb) else (2 if (not ma and not mb) else 0)
+                    table = (spr_i, spr_a, spr_b)[which]
                     la.append(l), a.append(s), lb.append(l2), b.append(s2), cy.append(c)
                     ev.append(np.asarray(d, float) / np.linalg.norm(d))
                     k0.append(table[(s, d)])
+                    src.append(which), key.append(self.key_index[(s, d)])
         self.bond_la, self.bond_a = np.array(la), np.array(a)
         self.bond_lb, self.bond_b = np.array(lb), np.array(b)
         self.bond_cy, self.bond_e, self.bond_k0 = np.array(cy), np.array(ev), np.array(k0)
+        self.bond_src, self.bond_key = np.array(src), np.array(key)
         # Parameters: the bonds nearest to the interface layer boundary (never
         # the half bonds at the device ends).
         mid = self.split - 0.5
@@ -135,6 +154,7 @@ class HeteroModel:
         self.is_param = np.zeros(self.bond_k0.size, dtype=bool)
         self.is_param[self.param_bonds] = True
         self.contrib = self._contributions()
+        self._lead_contrib = {m: self._lead_contributions(m) for m in ("A", "B")}
 
     # ---------------------------------------------------------------- blocks
     def _contributions(self) -> Contrib:
@@ -170,10 +190,28 @@ class HeteroModel:
         return Contrib(np.array(kind), np.array(layer), np.array(row), np.array(col), np.array(phase, float),
                        np.array(raw), np.array(ma), np.array(mb), np.array(bond))
 
-    def blocks(self, theta: torch.Tensor, kpoints, masses: torch.Tensor | None = None, device=None):
+    def spring_values(self, theta: torch.Tensor, phi_a: torch.Tensor | None = None,
+                      phi_b: torch.Tensor | None = None) -> torch.Tensor:
+        """Spring constant of every device bond: the material tables phi_a /
+        phi_b (default the model's) for A-A and B-B bonds and the half bonds
+        at the ends, the fixed interface table otherwise, theta on the
+        parameter bonds."""
+        dev = theta.device
+        kvals = torch.as_tensor(self.bond_k0, device=dev, dtype=torch.float64).clone()
+        for which, phi in ((1, phi_a), (2, phi_b)):
+            if phi is None:
+                continue
+            sel = np.flatnonzero(self.bond_src == which)
+            kvals = kvals.index_put((torch.as_tensor(sel, device=dev),),
+                                    phi.to(dev)[torch.as_tensor(self.bond_key[sel], device=dev)])
+        return kvals.index_put((torch.as_tensor(self.param_bonds, device=dev),), theta.to(dev))
+
+    def blocks(self, theta: torch.Tensor, kpoints, masses: torch.Tensor | None = None, device=None,
+               phi_a: torch.Tensor | None = None, phi_b: torch.Tensor | None = None):
         """(onsite [K, L, n, n], coupling [K, L-1, n, n]) complex128 for spring
-        values theta and device site masses ``masses`` ``[L, ny*nz]`` (default
-        the model's); differentiable in both with torch autograd.
+        values theta, material tables phi_a / phi_b and device site masses
+        ``masses`` ``[L, ny*nz]`` (defaults the model's); differentiable in all
+        of them with torch autograd.
 
         The spring contributions are summed with ``index_add``, which on a CUDA
         device adds in run-dependent order: the blocks, and T through them,
@@ -184,8 +222,7 @@ class HeteroModel:
         K, L, n = ky.numel(), self.L, self.n
         m = torch.as_tensor(self.mass, device=dev, dtype=torch.float64) if masses is None else masses.to(dev)
         mflat = m.reshape(-1)
-        kvals = torch.as_tensor(self.bond_k0, device=dev, dtype=torch.float64).clone()
-        kvals = kvals.index_put((torch.as_tensor(self.param_bonds, device=dev),), theta.to(dev))
+        kvals = self.spring_values(theta.to(dev), phi_a, phi_b)
         ct = self.contrib
         spring = kvals[torch.as_tensor(ct.bond, device=dev)]                      # [m]
         inv = torch.rsqrt(mflat[torch.as_tensor(ct.ma, device=dev)] * mflat[torch.as_tensor(ct.mb, device=dev)])
@@ -253,6 +290,77 @@ class HeteroModel:
                     else:
                         d01[ki, 3 * i:3 * i + 3, 3 * j:3 * j + 3] += w
         return {"d00": d00, "d01": d01, "d10": np.conj(np.swapaxes(d01, 1, 2)), "sites": sites}
+
+    def _lead_contributions(self, material: str) -> dict:
+        """Contribution table of the periodic lead's blocks, the same sums as
+        ``lead_blocks``: per term its block (0 d00, 1 d01), 3x3 offset, phase
+        shift, +-e e^T, the two masses (flat device index: layer 0 for A,
+        layer L-1 for B) and the material key of its spring."""
+        nz = self.nz_a if material == "A" else self.nz
+        sites = [(y, z) for y in range(self.ny) for z in range(nz)]
+        index = {st: i for i, st in enumerate(sites)}
+        lay = 0 if material == "A" else self.L - 1
+        t = {k: [] for k in ("blk", "row", "col", "phase", "raw", "ma", "mb", "key")}
+
+        def add(blk, row, col, phase, raw, ma, mb, key):
+            for k, v in zip(t, (blk, row, col, phase, raw, ma, mb, key)):
+                t[k].append(v)
+
+        for (y, z) in sites:
+            s_dev = y * self.nz + z
+            i = index[(y, z)]
+            for d in _half_space_neighbours():
+                dx, dy, dz = d
+                y2, z2 = y + dy, z + dz
+                if z2 < 0 or z2 >= nz:
+                    continue
+                c, y2 = divmod(y2, self.ny)
+                j = index[(y2, z2)]
+                e = np.asarray(d, float) / np.linalg.norm(d)
+                ee = np.outer(e, e)
+                key = self.key_index[(s_dev, d)]
+                fi, fj = lay * self.n_sites + s_dev, lay * self.n_sites + y2 * self.nz + z2
+                add(0, 3 * i, 3 * i, 0, ee, fi, fi, key)
+                add(0, 3 * j, 3 * j, 0, ee, fj, fj, key)
+                if dx == 0:
+                    add(0, 3 * i, 3 * j, c, -ee, fi, fj, key)
+                    add(0, 3 * j, 3 * i, -c, -ee, fj, fi, key)
+                else:
+                    add(1, 3 * i, 3 * j, c, -ee, fi, fj, key)
+        out = {k: np.array(v) for k, v in t.items()}
+        out["m"] = 3 * len(sites)
+        return out
+
+    def lead_blocks_torch(self, material: str, kpoints, phi: torch.Tensor | None = None,
+                          masses: torch.Tensor | None = None, device=None) -> dict:
+        """Lead A or B as torch tensors d00, d01, d10 = d01^H ``[K, m, m]``,
+        differentiable in its material table ``phi`` (default the model's)
+        and in the device masses (layer 0 for A, layer L-1 for B); equal to
+        ``lead_blocks`` at the defaults."""
+        dev = device or (phi.device if phi is not None else (masses.device if masses is not None else "cpu"))
+        ct = self._lead_contrib[material]
+        if phi is None:
+            phi = torch.as_tensor(self.phi0_a if material == "A" else self.phi0_b, device=dev)
+        m = torch.as_tensor(self.mass, device=dev, dtype=torch.float64) if masses is None else masses.to(dev)
+        mflat = m.reshape(-1)
+        ky = torch.as_tensor(np.array([k[0] for k in kpoints], float), device=dev)
+        K, mo = ky.numel(), ct["m"]
+        t = lambda a: torch.as_tensor(a, device=dev)  # noqa: E731
+        spring = phi.to(dev)[t(ct["key"])]
+        inv = torch.rsqrt(mflat[t(ct["ma"])] * mflat[t(ct["mb"])])
+        ph = torch.exp(1j * ky[:, None] * t(ct["phase"]).to(torch.float64)[None, :])
+        val = (spring * inv)[None, :, None, None] * ph[:, :, None, None] * t(ct["raw"])[None]
+        ar = torch.arange(3, device=dev)
+        r = t(ct["row"])[:, None, None] + ar[None, :, None]
+        c = t(ct["col"])[:, None, None] + ar[None, None, :]
+        flat = (r * mo + c).expand(-1, 3, 3)
+        out = []
+        for b in (0, 1):
+            sel = t(ct["blk"]) == b
+            blk = torch.zeros((K, mo * mo), dtype=torch.complex128, device=dev)
+            blk = blk.index_add(1, flat[sel].reshape(-1), val[:, sel].reshape(K, -1))
+            out.append(blk.reshape(K, mo, mo))
+        return {"d00": out[0], "d01": out[1], "d10": out[1].conj().transpose(-1, -2)}
 
     def omega_max(self, nk: int = 8) -> float:
         """Largest bulk phonon frequency of the two leads over a (kx, ky) sample."""

@@ -1,0 +1,209 @@
+"""Adjoint of the lead surface Green's functions: dkappa with respect to the
+lead force constants and masses, and to parameters shared by lead and device.
+
+The material spring tables phi_a and phi_b set the periodic leads and every
+A-A / B-B bond of the device, and the masses of device layers 0 and L-1 are
+also the lead masses, so these parameters reach kappa through both the
+decimated surface GFs and the device blocks.  The surface GFs are
+differentiated implicitly through their fixed point g = (z - H00 - H01 g H10)^-1
+(negfpy core/surface_gf.py:18-81 decimates to it), not through the decimation
+sweeps.  Checked against torch autograd through an unrolled torch decimation
+and a dense device solve (block order 24), and against central finite
+differences (h = 1e-6) of the forward kernels on 50 random lead parameters of
+the heterojunction (lead 48 | 30 layers of order 72 | lead 72).
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+from negfpy_b200 import adjoint  # noqa: E402
+from negfpy_b200.hetero import HeteroModel  # noqa: E402
+
+
+def sr_torch(z, d00, d01, tol=1e-12, maxiter=200):
+    """Sancho-Rubio decimation in torch (differentiable by unrolling), batched
+    over points: z [P], d00/d01 [P, n, n], d10 = d01^H."""
+    n = d00.shape[-1]
+    eye = torch.eye(n, dtype=torch.complex128, device=d00.device)
+    a, b = d01, d01.conj().transpose(-1, -2)
+    e = es = d00
+    for _ in range(maxiter):
+        g = torch.linalg.inv(z[:, None, None] * eye - e)
+        agb, bga = a @ g @ b, b @ g @ a
+        es, e = es + agb, e + agb + bga
+        a, b = a @ g @ a, b @ g @ b
+        if float(torch.maximum(a.abs().amax(), b.abs().amax())) < tol:
+            break
+    return torch.linalg.inv(z[:, None, None] * eye - es)
+
+
+def dense_kappa(pr, theta, masses, phi_a, phi_b):
+    """kappa from torch decimations of both leads and a dense device solve."""
+    m = pr.model
+    on, cp = m.blocks(theta, pr.kpoints, masses, phi_a=phi_a, phi_b=phi_b)
+    la, lb, vl, vr = pr.leads(masses, phi_a, phi_b)
+    K, L, n = on.shape[0], m.L, m.n
+    N = L * n
+    D = torch.zeros((K, N, N), dtype=torch.complex128, device=on.device)
+    for l in range(L):
+        D[:, l * n:(l + 1) * n, l * n:(l + 1) * n] = on[:, l]
+    for l in range(L - 1):
+        D[:, l * n:(l + 1) * n, (l + 1) * n:(l + 2) * n] = cp[:, l]
+        D[:, (l + 1) * n:(l + 2) * n, l * n:(l + 1) * n] = cp[:, l].conj().transpose(-1, -2)
+    ki = pr.ki.long()
+    z = (pr.omega + 1j * pr.eta) ** 2
+    g_l = sr_torch(z, la["d00"][ki], la["d01"][ki])
+    g_r = sr_torch(z, lb["d00"][ki], lb["d01"][ki])
+    sl = vl[ki] @ g_l @ vl[ki].conj().transpose(-1, -2)
+    sr = vr[ki] @ g_r @ vr[ki].conj().transpose(-1, -2)
+    eye = torch.eye(N, dtype=torch.complex128, device=on.device)
+    A = z[:, None, None] * eye - D[ki]
+    pad = torch.zeros_like(A)
+    pad[:, :n, :n] = sl
+    pad[:, N - n:, N - n:] = sr
+    A = A - pad
+    g = torch.linalg.solve(A, eye[:, N - n:].expand(A.shape[0], N, n))[:, :n, :]
+    gam_l = 1j * (sl - sl.conj().transpose(-1, -2))
+    gam_r = 1j * (sr - sr.conj().transpose(-1, -2))
+    t = torch.einsum("pab,pbc,pcd,pad->p", gam_l, g, gam_r, g.conj()).real
+    return pr.kappa_of_t(t.reshape(pr.W, pr.K))
+
+
+def _rel(a, b):
+    return float((a - b).abs().max()) / float(b.abs().max())
+
+
+@pytest.fixture(scope="module")
+def small():
+    model = HeteroModel(seed=7, ny=2, nz_a=2, nz_b=4, n_layers=6, n_params=60)
+    wmax = model.omega_max()
+    om = (np.arange(24) + 0.5) * (1.05 * wmax / 24)
+    kp = [(-2.0,), (0.3,), (2.9,)]
+    return adjoint.HeteroKappaProblem(model, kp, om, 1e-6 * wmax * wmax, 300.0, 2 * np.pi * 15e12 / wmax)
+
+
+def _params(pr, scale=0.0, seed=3):
+    m = pr.model
+    rng = np.random.default_rng(seed)
+    f = lambda x: torch.as_tensor(x * (1 + scale * rng.uniform(-1, 1, size=x.shape)), device="cuda")  # noqa: E731
+    return f(m.theta0), f(m.mass), f(m.phi0_a), f(m.phi0_b)
+
+
+def test_full_forward_matches_fixed_lead_path(small):
+    th, ms, pa, pb = _params(small)
+    k_full = small.kappa_full(th, ms, pa, pb)
+    k_fix = float(small.kappa_of_t(small.transmission_theta(th, ms)))
+    assert abs(k_full - k_fix) <= 1e-10 * abs(k_fix)
+
+
+@pytest.mark.parametrize("scale", [0.0, 0.05])
+def test_lead_grads_match_dense_autograd(small, scale):
+    th, ms, pa, pb = _params(small, scale)
+    kap, d_th, d_m, d_pa, d_pb = small.kappa_and_grad_all(th, ms, pa, pb)
+    leaves = [x.clone().requires_grad_(True) for x in (th, ms, pa, pb)]
+    kd = dense_kappa(small, *leaves)
+    r_th, r_m, r_pa, r_pb = torch.autograd.grad(kd, leaves)
+    assert abs(float(kap) - float(kd)) <= 1e-10 * abs(float(kd))
+    for a, b in ((d_th, r_th), (d_m, r_m), (d_pa, r_pa), (d_pb, r_pb)):
+        assert float(b.abs().max()) > 0
+        assert _rel(a, b) < 1e-8, _rel(a, b)
+    # the autograd primitive gives the same gradients
+    leaves2 = [x.clone().requires_grad_(True) for x in (th, ms, pa, pb)]
+    k2 = adjoint.kappa_all(leaves2[0], small, leaves2[1], leaves2[2], leaves2[3])
+    g2 = torch.autograd.grad(k2, leaves2)
+    for a, b in zip(g2, (r_th, r_m, r_pa, r_pb)):
+        assert _rel(a, b) < 1e-8
+
+
+def test_vjp_random_weights_matches_dense_autograd(small):
+    """A random-weight VJP of T through TransportFunction, lead blocks included."""
+    gen = torch.Generator(device="cpu").manual_seed(12)
+    th, ms, pa, pb = _params(small, 0.02, seed=9)
+    w = torch.randn((small.W, small.K), generator=gen, dtype=torch.float64).cuda()
+    la, lb, vl, vr = small.leads(ms, pa, pb)
+    blocks = [x.detach().clone().requires_grad_(True) for x in
+              (*small.model.blocks(th, small.kpoints, ms, phi_a=pa, phi_b=pb), vl, vr, la["d00"], la["d01"],
+               lb["d00"], lb["d01"])]
+    t = adjoint.TransportFunction.apply(*blocks, small._points())
+    g_adj = torch.autograd.grad(t, blocks, grad_outputs=w)
+    # reference: the same function of the same leaf blocks, densely
+    ref_leaves = [x.detach().clone().requires_grad_(True) for x in blocks]
+    pr = small
+
+    def dense_t(on, cp, vl_, vr_, l00, l01, r00, r01):
+        K, L, n = on.shape[0], pr.model.L, pr.model.n
+        N = L * n
+        D = torch.zeros((K, N, N), dtype=torch.complex128, device=on.device)
+        for l in range(L):
+            D[:, l * n:(l + 1) * n, l * n:(l + 1) * n] = on[:, l]
+        for l in range(L - 1):
+            D[:, l * n:(l + 1) * n, (l + 1) * n:(l + 2) * n] = cp[:, l]
+            D[:, (l + 1) * n:(l + 2) * n, l * n:(l + 1) * n] = cp[:, l].conj().transpose(-1, -2)
+        ki = pr.ki.long()
+        z = (pr.omega + 1j * pr.eta) ** 2
+        sl = vl_[ki] @ sr_torch(z, l00[ki], l01[ki]) @ vl_[ki].conj().transpose(-1, -2)
+        sr = vr_[ki] @ sr_torch(z, r00[ki], r01[ki]) @ vr_[ki].conj().transpose(-1, -2)
+        eye = torch.eye(N, dtype=torch.complex128, device=on.device)
+        A = z[:, None, None] * eye - D[ki]
+        pad = torch.zeros_like(A)
+        pad[:, :n, :n] = sl
+        pad[:, N - n:, N - n:] = sr
+        g = torch.linalg.solve(A - pad, eye[:, N - n:].expand(A.shape[0], N, n))[:, :n, :]
+        gl_ = 1j * (sl - sl.conj().transpose(-1, -2))
+        gr_ = 1j * (sr - sr.conj().transpose(-1, -2))
+        return torch.einsum("pab,pbc,pcd,pad->p", gl_, g, gr_, g.conj()).real.reshape(pr.W, pr.K)
+
+    g_ref = torch.autograd.grad(dense_t(*ref_leaves), ref_leaves, grad_outputs=w)
+    for a, b in zip(g_adj, g_ref):
+        assert _rel(a, b) < 1e-8, _rel(a, b)
+
+
+@pytest.fixture(scope="module")
+def hetero():
+    return adjoint.hetero_problem(n_k=4, n_omega=96)
+
+
+def test_hetero_lead_grads_match_central_differences(hetero):
+    m = hetero.model
+    assert m.n == 72 and m.n_a == 48 and m.L == 30
+    th, ms, pa, pb = _params(hetero)
+    kap, d_th, d_m, d_pa, d_pb = hetero.kappa_and_grad_all(th, ms, pa, pb)
+    assert abs(float(kap) - hetero.kappa_full(th, ms, pa, pb)) <= 1e-11 * abs(float(kap))
+    h = 1e-6
+    rng = np.random.default_rng(21)
+    # 50 lead parameters: 25 entries of each material table that the leads use
+    used_a = np.flatnonzero(d_pa.abs().cpu().numpy() > 0)
+    used_b = np.flatnonzero(d_pb.abs().cpu().numpy() > 0)
+    sel_a = rng.choice(used_a, size=25, replace=False)
+    sel_b = rng.choice(used_b, size=25, replace=False)
+    for phi, sel, grad, which in ((pa, sel_a, d_pa, "a"), (pb, sel_b, d_pb, "b")):
+        fd = []
+        for q in sel:
+            pp, pm = phi.clone(), phi.clone()
+            pp[q] += h
+            pm[q] -= h
+            args_p = (th, ms, pp, pb) if which == "a" else (th, ms, pa, pp)
+            args_m = (th, ms, pm, pb) if which == "a" else (th, ms, pa, pm)
+            fd.append((hetero.kappa_full(*args_p) - hetero.kappa_full(*args_m)) / (2 * h))
+        ga = grad.cpu().numpy()
+        err = np.abs(np.array(fd) - ga[sel]) / np.abs(ga).max()
+        assert float(err.max()) < 1e-5, (which, float(err.max()))
+    # masses shared by a lead and the device: layer 0 (lead A) and layer L-1 (lead B)
+    n_sites = m.n_sites
+    cand = np.concatenate([np.flatnonzero(m.active[0]), (m.L - 1) * n_sites + np.flatnonzero(m.active[m.L - 1])])
+    msel = rng.choice(cand, size=10, replace=False)
+    fdm = []
+    for q in msel:
+        mp, mm = ms.clone().reshape(-1), ms.clone().reshape(-1)
+        mp[q] += h
+        mm[q] -= h
+        fdm.append((hetero.kappa_full(th, mp.reshape(ms.shape), pa, pb)
+                    - hetero.kappa_full(th, mm.reshape(ms.shape), pa, pb)) / (2 * h))
+    gm = d_m.reshape(-1).cpu().numpy()
+    errm = np.abs(np.array(fdm) - gm[msel]) / np.abs(gm).max()
+    assert float(errm.max()) < 1e-5, float(errm.max())
