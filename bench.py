@@ -233,12 +233,15 @@ def fp64_peak_tflops(torch):
     return 2.0 * 8192 ** 3 / best / 1e12
 
 
-def refined_vs_f64(torch, omega_stride=1, parity_points=512, cores=None):
+def refined_vs_f64(torch, omega_stride=1, parity_points=512, cores=None, mixed_stride=4):
     """Plain FP64 and the refined pipeline on the 3D bulk workload (n = 96,
     16 x 16 k, 40 identical layers, 4096 omegas; every ``omega_stride``-th
-    omega), each timed with CUDA events over the whole grid.  kappa(300 K)
-    of the two is compared, and ``parity_points`` random points of the FP64
-    result are checked against the oracle (negfpy's algorithm) on the host."""
+    omega), each timed with CUDA events over the whole grid: FP64 surface GFs,
+    then the device solve from FP32 factors refined to FP64 accuracy, with the
+    FP64 re-solve of points whose refinement fails.  The unrefined FP32 sweep
+    ("mixed") is timed on every ``mixed_stride``-th of those omegas.  kappa(300 K)
+    of each is compared with FP64's, and ``parity_points`` random points of the
+    FP64 result are checked against the oracle (negfpy's algorithm) on the host."""
     from negfpy_b200 import engine, spectrum, workloads as Wm
     from negfpy_b200.adjoint import kappa_weights
     from oracle import negf_oracle as O
@@ -252,34 +255,57 @@ def refined_vs_f64(torch, omega_stride=1, parity_points=512, cores=None):
     om = om_w[w_idx].contiguous()
     eta = torch.full_like(om, wl.eta)
     warm = slice(0, 4 * K)
-    for prec in ("f64", "refined"):
+    for prec in ("f64", "refined", "mixed"):
         s.transmission(om[warm], k_idx[warm], eta[warm], precision=prec)
-    res, ms = {}, {}
-    for prec in ("f64", "refined"):
+
+    def timed(prec, sel):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
         e0.record()
-        res[prec] = s.transmission(om, k_idx, eta, precision=prec)
+        r = s.transmission(om[sel], k_idx[sel], eta[sel], precision=prec)
         e1.record()
         torch.cuda.synchronize()
-        ms[prec] = e0.elapsed_time(e1)
+        return r, e0.elapsed_time(e1)
+
     P = int(om.numel())
+    allp = slice(0, P)
+    res, ms = {}, {}
+    for prec in ("f64", "refined"):
+        res[prec], ms[prec] = timed(prec, allp)
+    wm = np.arange(0, len(wi), mixed_stride)
+    msel = torch.as_tensor((wm[:, None] * K + np.arange(K)[None, :]).ravel(), device="cuda")
+    res["mixed"], ms["mixed"] = timed("mixed", msel)
     w = kappa_weights(om_w, 300.0, wl.omega_unit_rad_s)
-    kap = {p: float((w * res[p]["T"].reshape(len(wi), K).mean(1)).sum()) for p in res}
+    wmix = kappa_weights(om_w[torch.as_tensor(wm, device="cuda")], 300.0, wl.omega_unit_rad_s)
+    kap = {p: float((w * res[p]["T"].reshape(len(wi), K).mean(1)).sum()) for p in ("f64", "refined")}
     t64, tr = res["f64"]["T"], res["refined"]["T"]
     tb64 = t64.reshape(len(wi), K).mean(1)
     tbr = tr.reshape(len(wi), K).mean(1)
     per_w = ((tbr - tb64).abs() / tb64.abs().clamp_min(1.0)).cpu().numpy()
+    t64m = t64[msel]
+    k64m = float((wmix * t64m.reshape(len(wm), K).mean(1)).sum())
+    kmix = float((wmix * res["mixed"]["T"].reshape(len(wm), K).mean(1)).sum())
+    steps = res["refined"]["steps"].cpu().numpy()
+    Pm = int(msel.numel())
     out = {"workload": f"bulk_n96_L40_K256, {len(wi)} of 4096 omegas ({P} points)",
-           "Tbar_err_per_omega": {"max": float(per_w.max()), "median": float(np.median(per_w)),
-                                  "p99": float(np.quantile(per_w, 0.99))},
            "f64_points_per_s": P / ms["f64"] * 1e3, "refined_points_per_s": P / ms["refined"] * 1e3,
            "f64_s": ms["f64"] / 1e3, "refined_s": ms["refined"] / 1e3,
            "speedup": ms["f64"] / ms["refined"], "kappa_rel_err": (kap["refined"] - kap["f64"]) / kap["f64"],
+           "Tbar_err_per_omega": {"max": float(per_w.max()), "median": float(np.median(per_w)),
+                                  "p99": float(np.quantile(per_w, 0.99))},
            "T_max_rel_err": float(((tr - t64).abs() / t64.abs().clamp_min(1.0)).max()),
            "fallback_points": int(res["refined"]["fallback"]),
-           "method": "FP64 Sancho-Rubio; device sweep FP32 on 3xTF32 mma.sync with FP64 Sigma/Gamma/trace; "
-                     "FP64 re-solve of failed points"}
+           "refine_steps": {"mean": float(steps.mean()), "max": int(steps.max()),
+                            "histogram": {str(k): int((steps == k).sum()) for k in np.unique(steps)}},
+           "method": "FP64 Sancho-Rubio; device solve: FP32 block LU (3xTF32 mma.sync, FP32 Gauss-Jordan) refined "
+                     "to FP64 accuracy (FP64 DMMA residuals, stop when the predicted next correction of G_0,L-1 is "
+                     "<= 1e-12), FP64 re-solve of NEGF_REFINE_FAIL points",
+           "mixed_unrefined": {"workload": f"every {mixed_stride}th of those omegas ({Pm} points)",
+                               "points_per_s": Pm / ms["mixed"] * 1e3,
+                               "speedup_vs_f64": (Pm / ms["mixed"]) / (P / ms["f64"]),
+                               "kappa_rel_err": (kmix - k64m) / k64m,
+                               "T_max_rel_err": float(((res["mixed"]["T"] - t64m).abs()
+                                                       / t64m.abs().clamp_min(1.0)).max())}}
     if parity_points:
         cores = cores or os.cpu_count() or 1
         rng = np.random.default_rng(11)
@@ -363,22 +389,50 @@ def grad_vs_forward(torch, n_k=8, n_omega=256, reps=3):
     g1.record()
     torch.cuda.synchronize()
     grad = g0.elapsed_time(g1) / reps
+    # Leads as variables: both material tables and the masses reach the
+    # lead blocks, so the forward decimates both leads again and the gradient
+    # adds the surface-GF adjoints.
+    th = theta
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    pr.kappa_full(th)
+    pr.kappa_and_grad_all(th)
+    torch.cuda.synchronize()
+    f0.record()
+    for _ in range(reps):
+        pr.kappa_full(th)
+    f1.record()
+    torch.cuda.synchronize()
+    fwd_all = f0.elapsed_time(f1) / reps
+    g0.record()
+    for _ in range(reps):
+        pr.kappa_and_grad_all(th)
+    g1.record()
+    torch.cuda.synchronize()
+    grad_all = g0.elapsed_time(g1) / reps
+    m = pr.model
     return {"workload": f"heterojunction lead48|L30 n72|lead72, 2000 spring params + 720 site masses, "
                         f"{n_omega} omega x {n_k} k",
             "forward_ms": fwd, "grad_ms": grad, "grad_over_forward": grad / fwd,
             "lead_sgf_ms_once": e[0].elapsed_time(e[1]),
             "note": "forward = theta -> blocks -> device solve -> kappa; grad = dkappa/dtheta and dkappa/dmasses "
                     "from one adjoint launch (forward sweeps recomputed inside) + autograd through the block "
-                    "builder; lead GFs do not depend on theta"}
+                    "builder; lead GFs do not depend on theta",
+            "with_leads": {"params": f"theta (2000) + masses (720) + material tables A and B "
+                                     f"({m.phi0_a.size} + {m.phi0_b.size}), shared by leads and device",
+                           "forward_ms": fwd_all, "grad_ms": grad_all, "grad_over_forward": grad_all / fwd_all,
+                           "note": "forward = leads and device blocks rebuilt, both leads decimated, device solve, "
+                                   "kappa; grad = both decimations + one device adjoint launch with the contact "
+                                   "self-energy adjoints + one surface-GF adjoint launch per lead (implicit, no "
+                                   "differentiation through the sweeps) + autograd through the block builders"}}
 
 
 def uneven_batch(torch, omega_stride=16):
     """The uneven batch (64 seeded systems, n in {24..192}, 10-60 layers,
     1-256 k, 1024 omegas each) on every ``omega_stride``-th omega of each
     system: autotuned launch shape and item order, one persistent launch per
-    solve replayed from a CUDA graph, FP64 and refined (mixed device sweep with
-    FP64 re-solve of failed items).  Reports points/s of both and the
-    per-system kappa(300 K) error of the refined result against FP64."""
+    solve replayed from a CUDA graph, FP64 and mixed (FP32 device sweep without
+    refinement, FP64 re-solve of failed items).  Reports points/s of both and
+    the per-system kappa(300 K) error of the mixed result against FP64."""
     from negfpy_b200 import workloads as Wm
     from negfpy_b200.adjoint import kappa_weights
     from negfpy_b200.autotune import BatchTuner
@@ -437,7 +491,7 @@ def uneven_batch(torch, omega_stride=16):
     errs = np.abs(np.array(errs))
     return {"workload": f"64 systems, n in {{24..192}}, L 10-60, K 1-256, every {omega_stride}th of 1024 omegas "
                         f"({int(offs[-1])} points)",
-            "f64": out["f64"], "refined": out["mixed"],
+            "f64": out["f64"], "mixed": out["mixed"],
             "speedup": out["mixed"]["points_per_s"] / out["f64"]["points_per_s"],
             "kappa_rel_err_max": float(errs.max()), "kappa_rel_err_median": float(np.median(errs)),
             "launch": "one persistent kernel per solve, replayed from a CUDA graph; shape and order autotuned"}

@@ -190,9 +190,10 @@ size_t negf_rgf_refined_workspace_bytes(int n_dev, int n_lead_l, int n_lead_r, i
  * tol, max_steps and steps_out.  The block LU factors of A come from an FP32
  * sweep (3 x TF32 tensor-core products, FP32 Gauss-Jordan); the right-contact
  * block column X is then refined: R = E_R - A X in FP64, A d = R solved with
- * the FP32 factors, X += d.  It stops after the first step k whose relative
- * correction of X_0 = G_{0,L-1}, nu_k, satisfies nu_k^2 / nu_{k-1} <= tol
- * (nu_0 = 1).  A point whose correction fails to halve from one step to the
+ * the FP32 factors, X += d.  With nu_k = max|d| / max|X| over all blocks
+ * after step k, it stops at the first k >= 2 with nu_k^2 / nu_{k-1} <= tol
+ * (the next correction predicted from the measured contraction), or when
+ * nu_k <= tol.  A point whose correction fails to halve from one step to the
  * next, or that does not converge within max_steps, reports
  * NEGF_REFINE_FAIL; a singular or non-finite FP32 pivot NEGF_SINGULAR /
  * NEGF_NONFINITE.  The caller re-solves those points with

@@ -10,8 +10,10 @@ per (omega, k)); an item is (system, k index, omega).  The host
   persistent blocks finish together),
 * launches once, optionally inside a CUDA graph that is replayed for repeated
   solves of the same items,
-* for ``precision="refined"`` re-solves in FP64 the items whose FP32 device
-  sweep failed.
+* for ``precision="mixed_fallback"`` re-solves in FP64 the items whose FP32
+  device sweep failed.  (The batch kernel has no iterative refinement: its
+  mixed result carries FP32-level error; ``engine.StackedSystem`` with
+  ``precision="refined"`` is the FP64-accurate reduced-precision solve.)
 
 Launch shapes (blocks per SM) and the item order come from
 ``negfpy_b200.autotune``.
@@ -208,14 +210,14 @@ class UnevenBatch:
     def solve(self, it: Items, precision: str = "f64", grid: int = 0, tol: float = 1e-12,
               maxiter: int = 200, blocks_per_sm: int = 1) -> dict:
         """T, status and sweeps in the CALLER's item order.  ``precision``:
-        "f64", "mixed", or "refined" (mixed, then the FP64 re-solve of the
-        items whose device sweep failed while their leads converged)."""
-        if precision not in ("f64", "mixed", "refined"):
-            raise ValueError(f"unknown precision {precision!r}; expected 'f64', 'mixed' or 'refined'")
+        "f64", "mixed", or "mixed_fallback" (mixed, then the FP64 re-solve of
+        the items whose device sweep failed while their leads converged)."""
+        if precision not in ("f64", "mixed", "mixed_fallback"):
+            raise ValueError(f"unknown precision {precision!r}; expected 'f64', 'mixed' or 'mixed_fallback'")
         T, st, iters = self.launch(it, "f64" if precision == "f64" else "mixed", grid, tol, maxiter,
                                    blocks_per_sm=blocks_per_sm)
         n_fallback = 0
-        if precision == "refined":
+        if precision == "mixed_fallback":
             bad = (st == _lib.SINGULAR) | (st == _lib.NONFINITE)
             idx = torch.nonzero(bad).flatten()
             n_fallback = int(idx.numel())

@@ -434,7 +434,7 @@ __device__ void gemm_add(double2* dst, const double2* A, const double2* B, int N
 // is summed by doubling (Smith's method): Lam += A Lam B, A <- A^2, B <- B^2
 // from A = Q, B = P, until max(max|A|, max|B|) < tol; no inverse is needed and
 // nothing is differentiated through the decimation sweeps.  Then
-//   H00bar = g Lam g,  H01bar = g H10 H00bar,  H10bar = H00bar P,
+//   H00bar = g Lam g,  H01bar = g H10 H00bar,  H10bar = H00bar H01 g,
 // added into the per-k accumulators (with H10 = H01^H, H10bar^H is added to
 // H01bar instead).  Status: kMaxIter if the doubling does not converge within
 // maxiter, kNonFinite on inf/nan.
@@ -532,7 +532,8 @@ __global__ void __launch_bounds__(kThreads, 2) sgf_adjoint_f64_kernel(SgfAdjArgs
       if (h10) gemm_to<false, false>(Tt, Gb, H10b, NP, kl);   // g H10
       else gemm_to<false, true>(Tt, Gb, H01b, NP, kl);
       gemm_to<false, false>(T2, Tt, T1, NP, kl);     // H01bar = g H10 H00bar
-      gemm_to<false, false>(Tt, T1, Pk, NP, kl);     // H10bar = H00bar P
+      gemm_to<false, false>(Aq2, H01b, Gb, NP, kl);  // H01 g
+      gemm_to<false, false>(Tt, T1, Aq2, NP, kl);    // H10bar = H00bar H01 g
       double2* g00 = sa.grad_h00 + k * (long long)nl * nl;
       double2* g01 = sa.grad_h01 + k * (long long)nl * nl;
       double2* g10 = sa.grad_h10 ? sa.grad_h10 + k * (long long)nl * nl : nullptr;

@@ -16,12 +16,13 @@
 //     products per layer), the correction A d = R with the FP32 factors
 //     (forward y_i = g_i (R_i + C_{i-1}^H y_{i-1}), backward
 //     d_i = y_i + g_i C_i d_{i+1}), X += d in FP64.  With
-//     nu_k = max|d_0| / max|X_0| after step k, the step count is the smallest
-//     k with nu_k^2 / nu_{k-1} <= tol (nu_0 = 1): the next correction, which
-//     shrinks by the same factor, is then below tol.  A step whose
-//     correction did not shrink to half the previous one, or no convergence
-//     within maxit steps, gives NEGF_REFINE_FAIL for the point (the host
-//     solves those points again in FP64).
+//     nu_k = max|d| / max|X| over all blocks after step k and the measured
+//     contraction rho_k = nu_k / nu_{k-1}, the refinement stops at the first
+//     k >= 2 with nu_k rho_k <= tol (the next correction, predicted from the
+//     contraction, is below tol), or as soon as nu_k <= tol.  A step whose
+//     correction did not shrink to half the previous one (rho_k > 1/2), or
+//     no convergence within maxit steps, gives NEGF_REFINE_FAIL for the point
+//     (the host solves those points again in FP64).
 //  4. Gamma_L, Gamma_R and the trace in FP64 from X_0 = G_{0,L-1}.
 #include "negf_common.cuh"
 #include "negf_f64.h"
@@ -188,7 +189,7 @@ static __device__ int refine_point(const glob::RgfPoint& q, int NP, unsigned cha
   __syncthreads();
 
   // 3. Refinement.
-  double nu_prev = 1.0;
+  double nu_prev = 0.0;
   bool done = false;
   for (int it = 1; it <= maxit && !done; ++it) {
     *steps = it;
@@ -277,10 +278,8 @@ static __device__ int refine_point(const glob::RgfPoint& q, int NP, unsigned cha
             if (r < n && cc < n) {
               const double2 x = cadd(Xi[e], make_double2((double)d.x, (double)d.y));
               Xi[e] = x;
-              if (i == 0) {
-                dmax = fmax(dmax, fmax(fabs((double)d.x), fabs((double)d.y)));
-                xmax = fmax(xmax, fmax(fabs(x.x), fabs(x.y)));
-              }
+              dmax = fmax(dmax, fmax(fabs((double)d.x), fabs((double)d.y)));
+              xmax = fmax(xmax, fmax(fabs(x.x), fabs(x.y)));
             }
           }
       }
@@ -294,11 +293,15 @@ static __device__ int refine_point(const glob::RgfPoint& q, int NP, unsigned cha
     dmax = block_max(dmax, red);
     xmax = block_max(xmax, red);
     const double nu = xmax > 0.0 ? dmax / xmax : 0.0;
-    if (nu * nu <= tol * nu_prev || nu <= tol) {
+    if (nu <= tol) {
       done = true;
-    } else if (nu > 0.5 * nu_prev) {
-      status = kRefineFail;  // the correction stopped shrinking
-      break;
+    } else if (it >= 2) {
+      const double rho = nu / nu_prev;
+      if (rho > 0.5) {
+        status = kRefineFail;  // the correction stopped shrinking
+        break;
+      }
+      if (nu * rho <= tol) done = true;
     }
     nu_prev = nu;
   }

@@ -132,7 +132,7 @@ def rgf_transmission(onsite: torch.Tensor, coupling: torch.Tensor | None, n_laye
 
 
 REFINE_TOL = 1e-12
-REFINE_MAX_STEPS = 4
+REFINE_MAX_STEPS = 5
 
 
 def rgf_transmission_refine64(onsite, coupling, n_layers, vl, vr, gl, gr, omega, eta_dev, k_index, lead_status,

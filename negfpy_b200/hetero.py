@@ -56,6 +56,18 @@ class Contrib:
     bond: np.ndarray    # bond index
 
 
+class _deterministic:
+    """Within the block builders, scatter-adds (index_add) in a fixed order on
+    the GPU too, so that equal parameters give bitwise-equal blocks."""
+
+    def __enter__(self):
+        self.prev = torch.are_deterministic_algorithms_enabled()
+        torch.use_deterministic_algorithms(True, warn_only=True)
+
+    def __exit__(self, *exc):
+        torch.use_deterministic_algorithms(self.prev)
+
+
 class HeteroModel:
     def __init__(self, seed: int = 4, ny: int = 2, nz_a: int = 8, nz_b: int = 12, n_layers: int = 30,
                  n_params: int = 2000, pin: float = 100.0):
@@ -213,10 +225,12 @@ class HeteroModel:
         ``masses`` ``[L, ny*nz]`` (defaults the model's); differentiable in all
         of them with torch autograd.
 
-        The spring contributions are summed with ``index_add``, which on a CUDA
-        device adds in run-dependent order: the blocks, and T through them,
-        vary at rounding level between runs unless
-        ``torch.use_deterministic_algorithms(True)`` is set."""
+        The spring contributions are summed with ``index_add`` in torch's
+        deterministic mode, so equal parameters give bitwise-equal blocks."""
+        with _deterministic():
+            return self._blocks(theta, kpoints, masses, device, phi_a, phi_b)
+
+    def _blocks(self, theta, kpoints, masses, device, phi_a, phi_b):
         dev = device or theta.device
         ky = torch.as_tensor(np.array([k[0] for k in kpoints], float), device=dev)
         K, L, n = ky.numel(), self.L, self.n
@@ -336,7 +350,11 @@ class HeteroModel:
         """Lead A or B as torch tensors d00, d01, d10 = d01^H ``[K, m, m]``,
         differentiable in its material table ``phi`` (default the model's)
         and in the device masses (layer 0 for A, layer L-1 for B); equal to
-        ``lead_blocks`` at the defaults."""
+        ``lead_blocks`` at the defaults.  Summed in torch's deterministic mode."""
+        with _deterministic():
+            return self._lead_blocks_torch(material, kpoints, phi, masses, device)
+
+    def _lead_blocks_torch(self, material, kpoints, phi, masses, device):
         dev = device or (phi.device if phi is not None else (masses.device if masses is not None else "cpu"))
         ct = self._lead_contrib[material]
         if phi is None:

@@ -1,5 +1,5 @@
 """Uneven batch in one persistent launch: every item against the per-system
-FP64 path and a sample against the oracle, the refined precision against
+FP64 path and a sample against the oracle, the mixed precision against
 FP64, CUDA-graph replay, out-of-range items, a system with different leads,
 and the autotuner on the GPU."""
 
@@ -67,11 +67,11 @@ def test_batch_matches_oracle_sample(small):
             assert abs(got - ref) <= TOL_T * max(1.0, abs(ref)), (si, wi, ki, got, ref)
 
 
-def test_batch_refined_against_f64(small):
+def test_batch_mixed_against_f64(small):
     ws, b = small
     it = b.items([w.omegas for w in ws], "lpt")
     r64 = b.solve(it, "f64")
-    rr = b.solve(it, "refined")
+    rr = b.solve(it, "mixed_fallback")
     assert int((rr["status"] != 0).sum()) == 0
     err = float(((rr["T"] - r64["T"]).abs() / r64["T"].abs().clamp_min(1.0)).max())
     assert err <= 1e-3, err

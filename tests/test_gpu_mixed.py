@@ -72,21 +72,21 @@ def test_mixed_heterojunction_layer_resolved():
     assert err <= 1e-3, err
 
 
-def test_refined_fallback_and_lead_status():
+def test_mixed_fallback_and_lead_status():
     wl = W.slab_workload()
     wi = np.arange(5, wl.omegas.size, 256)
     t64, tm, args = _both(wl, wi)
-    t, st, nb = engine.rgf_transmission_refined(*args)
+    t, st, nb = engine.rgf_transmission_mixed(*args)
     assert nb == 0 and int((st != 0).sum()) == 0
     assert torch.equal(t, tm)
     # a failed lead skips the point and keeps its status; it is not re-solved
     lst = args[-1].clone()
     lst[3] = 1
-    t2, st2, nb2 = engine.rgf_transmission_refined(*args[:-1], lst)
+    t2, st2, nb2 = engine.rgf_transmission_mixed(*args[:-1], lst)
     assert nb2 == 0 and int(st2[3]) == 1 and bool(torch.isnan(t2[3]))
     s = engine.StackedSystem.from_arrays(wl.lead_l, wl.lead_l, wl.onsite, wl.coupling, wl.n_layers, same_leads=True)
     om, ki, eta = _points(wl, wi)
-    r = s.transmission(om, ki, eta, precision="refined")
+    r = s.transmission(om, ki, eta, precision="mixed")
     assert r["fallback"] == 0 and torch.equal(r["T"], tm)
 
 
