@@ -512,7 +512,7 @@ def profile_case(name, torch):
         w_idx, k_idx = spectrum.grid_points(len(wi), K, om_w.device)
         om = om_w[w_idx].contiguous()
         eta = torch.full_like(om, wl.eta)
-        e = [ev() for _ in range(4)]
+        e = [ev() for _ in range(5)]
         e[0].record()
         rl = engine.sgf_sr(*s.lead_l, om, eta, k_idx)
         e[1].record()
@@ -522,22 +522,29 @@ def profile_case(name, torch):
         engine.rgf_transmission(s.onsite, s.coupling, s.n_layers, s.vl, s.vr, rl["g"], rl["g"], om, eta, k_idx,
                                 rl["status"], precision="mixed")
         e[3].record()
+        _, _, steps = engine.rgf_transmission_refine64(s.onsite, s.coupling, s.n_layers, s.vl, s.vr, rl["g"],
+                                                       rl["g"], om, eta, k_idx, rl["status"])
+        e[4].record()
         torch.cuda.synchronize()
         out.update(points=int(om.numel()), sr_ms=e[0].elapsed_time(e[1]), rgf_f64_ms=e[1].elapsed_time(e[2]),
-                   rgf_mixed_ms=e[2].elapsed_time(e[3]))
+                   rgf_mixed_ms=e[2].elapsed_time(e[3]), rgf_refined_ms=e[3].elapsed_time(e[4]),
+                   refine_steps_mean=float(steps.float().mean()))
     elif name == "grad":
         from negfpy_b200 import adjoint
 
         pr = adjoint.hetero_problem(n_k=4, n_omega=32)
         theta = torch.as_tensor(pr.model.theta0, device="cuda")
-        e = [ev() for _ in range(3)]
+        e = [ev() for _ in range(4)]
         e[0].record()
         pr.transmission_theta(theta)
         e[1].record()
         pr.kappa_and_grad(theta)
         e[2].record()
+        pr.kappa_and_grad_all(theta)
+        e[3].record()
         torch.cuda.synchronize()
-        out.update(points=pr.W * pr.K, forward_ms=e[0].elapsed_time(e[1]), grad_ms=e[1].elapsed_time(e[2]))
+        out.update(points=pr.W * pr.K, forward_ms=e[0].elapsed_time(e[1]), grad_ms=e[1].elapsed_time(e[2]),
+                   grad_with_leads_ms=e[2].elapsed_time(e[3]))
     elif name == "batch":
         from negfpy_b200.batch import UnevenBatch
 

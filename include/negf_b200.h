@@ -211,6 +211,20 @@ int negf_rgf_transmission_refined(int n_dev, int n_lead_l, int n_lead_r, int n_l
                                   double tol, int max_steps, double* t_out, int* status_out, int* steps_out,
                                   void* workspace, size_t workspace_bytes, void* stream);
 
+/*
+ * Batched complex FP32 products on the fifth-generation tensor cores:
+ * c[p] = op(a[p]) op(b[p]) for batch independent n x n matrices (complex64,
+ * interleaved re, im, row-major, consecutive), op the conjugate transpose
+ * when conj_a / conj_b is nonzero.  Each real product is split 3 x TF32
+ * (tcgen05.mma kind::tf32, accumulators in Tensor Memory).  No counterpart
+ * in negfpy: the building block of the FP32 device sweeps, exposed so that
+ * it can be checked on its own.  n a multiple of 16 up to 128 (else
+ * NEGF_EUNSUPPORTED).  status_out[p] (may be NULL): NEGF_OK, or
+ * NEGF_NONFINITE if the product's completion wait ran out.
+ */
+int negf_cgemm_tf32x3(int n, int batch, const float* a, const float* b, float* c, int conj_a, int conj_b,
+                      int* status_out, void* stream);
+
 /* Workspace bytes negf_rgf_adjoint_f64 needs (0 on a bad size). */
 size_t negf_adjoint_workspace_bytes(int n_dev, int n_lead_l, int n_lead_r, int n_layers);
 

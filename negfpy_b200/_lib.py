@@ -56,6 +56,7 @@ _SIGNATURES = {
         [_I, _I, _I, _I, _I, _P, _LL, _LL, _P, _LL, _LL, _P, _LL, _P, _LL, _P, _LL, _P, _LL, _P, _P, _P, _P, _D,
          _I, _P, _P, _P, _P, _SZ, _P],
     ),
+    "negf_cgemm_tf32x3": (_I, [_I, _I, _P, _P, _P, _I, _I, _P, _P]),
     "negf_batch_max_grid": (_I, [_I, _I, _I]),
     "negf_batch_workspace_bytes": (_SZ, [_I, _I, _I, _I]),
     "negf_batch_system_bytes": (_SZ, []),

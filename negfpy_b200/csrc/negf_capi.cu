@@ -318,6 +318,19 @@ int negf_rgf_transmission_refined(int n_dev, int n_lead_l, int n_lead_r, int n_l
   return 0;
 }
 
+int negf_cgemm_tf32x3(int n, int batch, const float* a, const float* b, float* c, int conj_a, int conj_b,
+                      int* status_out, void* stream) {
+  if (batch < 0 || n <= 0) return fail(NEGF_EINVAL, "negf_cgemm_tf32x3: sizes must be positive");
+  if (n % 16 != 0 || n > 128)
+    return fail(NEGF_EUNSUPPORTED, "negf_cgemm_tf32x3: n must be a multiple of 16 up to 128");
+  if (!a || !b || !c) return fail(NEGF_EINVAL, "negf_cgemm_tf32x3: null pointer");
+  if (batch == 0) return 0;
+  if (negf::tc_cgemm_launch(n, batch, reinterpret_cast<const float2*>(a), reinterpret_cast<const float2*>(b),
+                            reinterpret_cast<float2*>(c), conj_a, conj_b, status_out, as_stream(stream)) != 0)
+    return cuda_fail("negf_cgemm_tf32x3");
+  return 0;
+}
+
 int negf_batch_max_grid(int max_order, int precision, int blocks_per_sm) {
   if (max_order <= 0 || max_order > 256 || (precision != 0 && precision != 1)) return 0;
   if (blocks_per_sm != 1 && blocks_per_sm != 2) return 0;

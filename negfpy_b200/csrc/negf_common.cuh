@@ -48,6 +48,18 @@ __device__ __forceinline__ double2 crecip(double2 v) {
 __device__ __forceinline__ double cabs2(double2 a) { return a.x * a.x + a.y * a.y; }
 __device__ __forceinline__ bool cfinite(double2 a) { return isfinite(a.x) && isfinite(a.y); }
 
+// FP32 -> TF32 with round-to-nearest (ties away), as a bit pattern.
+__device__ __forceinline__ unsigned tf32_rna(float x) {
+  unsigned r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return r;
+}
+// x = hi + lo with both parts representable in TF32.
+__device__ __forceinline__ void split_tf32(float x, unsigned& hi, unsigned& lo) {
+  hi = tf32_rna(x);
+  lo = tf32_rna(x - __uint_as_float(hi));
+}
+
 // Single precision counterparts for the mixed-precision kernels.
 __device__ __forceinline__ void cfma(float2& acc, float2 a, float2 b) {
   acc.x = fmaf(a.x, b.x, acc.x);

@@ -112,11 +112,18 @@ int rgf_mixed_grid(int np);
 size_t rgf_mixed_ws_bytes(int np, int n, int grid);
 int rgf_mixed_launch(const RgfArgs& a, int np, int grid, void* ws, cudaStream_t st);
 
+namespace mixed {
+bool use_tc(int np);  // tcgen05 products at this padded order (<= 128, unless NEGF_TC=0)
+}
 // Refined device solve (FP32 factors, FP64 iterative refinement), orders 1..256.
 int rgf_refine_grid(int np);
 size_t rgf_refine_ws_bytes(int np, int n, int L, int grid);
 int rgf_refine_launch(const RgfArgs& a, int np, int grid, void* ws, double tol, int maxit, int* steps_out,
                       cudaStream_t st);
+
+// Batched complex FP32 products on tcgen05 (negf_tc.cu), n a multiple of 16 up to 128.
+int tc_cgemm_launch(int np, int batch, const float2* a, const float2* b, float2* c, int conj_a, int conj_b,
+                    int* status, cudaStream_t st);
 
 // Uneven batch (negf_batch.cu).
 int batch_max_grid(int npmax, int mixed, int minb);

@@ -18,6 +18,8 @@
 //
 // A point whose FP32 sweep meets a singular or non-finite pivot reports the
 // status; the host re-solves those points with the FP64 kernel.
+#include <cstdlib>
+
 #include "negf_common.cuh"
 #include "negf_f64.h"
 #include "negf_mixed.cuh"
@@ -26,13 +28,31 @@
 namespace negf {
 namespace mixed {
 
-__global__ void __launch_bounds__(kThreads) rgf_mixed_kernel(RgfArgs a, int NP, unsigned char* ws) {
-  extern __shared__ __align__(16) unsigned char smraw[];
-  const GJS32 sh = carve32(smraw, NP);
-  double* red = reinterpret_cast<double*>(smraw + ((gjs32_bytes(NP) + 15) / 16) * 16);
+// Dynamic shared memory: [tcgen05 stage and mbarrier (TC only) | GJ panel,
+// pivot bookkeeping | reduction scratch].  With TC at least 80 KB, so that at
+// most two blocks share an SM and their TMEM (2 x 256 columns) always fits.
+__host__ __device__ inline size_t tc_bytes(int np) { return ((tc::stage_bytes(np) + 16 + 127) / 128) * 128; }
+template <bool TC>
+size_t mixed_smem(int np) {
+  const size_t base = ((gjs32_bytes(np) + 15) / 16) * 16 + 40 * 8;
+  if (!TC) return base;
+  const size_t need = tc_bytes(np) + base;
+  return need > 80 * 1024 ? need : 80 * 1024;
+}
+
+template <bool TC>
+__global__ void __launch_bounds__(kThreads, 2) rgf_mixed_kernel(RgfArgs a, int NP, unsigned char* ws) {
+  extern __shared__ __align__(128) unsigned char smraw[];
+  unsigned char* gj = smraw + (TC ? tc_bytes(NP) : 0);
+  const GJS32 sh = carve32(gj, NP);
+  double* red = reinterpret_cast<double*>(gj + ((gjs32_bytes(NP) + 15) / 16) * 16);
   __shared__ int s_point;
+  __shared__ uint32_t s_tmem;
+  __shared__ int s_tcerr;
   const int n = a.n, tid = threadIdx.x;
   unsigned char* blk = ws + (long long)blockIdx.x * mixed_ws_bytes_per_block(NP, n);
+  tc::Ctx tcx;
+  if constexpr (TC) tcx = tc::setup(smraw, NP, &s_tmem, &s_tcerr);
 
   for (;;) {
     if (tid == 0) s_point = (int)atomicAdd(a.counter, 1u);
@@ -64,16 +84,27 @@ __global__ void __launch_bounds__(kThreads) rgf_mixed_kernel(RgfArgs a, int NP, 
     q.gR = a.gR + (long long)p * a.gr_ps;
     q.z = glob::z_of(a.omega[p], a.eta_dev[p]);
     double tval = 0.0;
-    const int status = rgf_point_mixed(q, NP, blk, sh, red, &tval);
+    const int status = rgf_point_mixed<TC>(q, NP, blk, sh, red, &tval, &tcx);
     if (tid == 0) {
       a.T_out[p] = (status == kOk) ? tval : __longlong_as_double(0x7ff8000000000000ULL);
       if (a.status_out) a.status_out[p] = status;
     }
     __syncthreads();
   }
+  if constexpr (TC) tc::teardown(tcx);
 }
 
-size_t mixed_smem_bytes(int np) { return ((gjs32_bytes(np) + 15) / 16) * 16 + 40 * 8; }
+}  // namespace mixed
+
+// tcgen05 products for orders up to 128 unless NEGF_TC=0 (kept for A/B timing).
+namespace mixed {
+bool use_tc(int np) {
+  static const int env = [] {
+    const char* v = getenv("NEGF_TC");
+    return (v && v[0] == '0') ? 0 : 1;
+  }();
+  return env && np <= tc::kMaxNP;
+}
 
 }  // namespace mixed
 
@@ -82,14 +113,14 @@ int mixed_order(int n) {
   return (n + 15) / 16 * 16;
 }
 int rgf_mixed_grid(int np) {
-  const size_t sm = mixed::mixed_smem_bytes(np);
-  if (cudaFuncSetAttribute(mixed::rgf_mixed_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) !=
-      cudaSuccess)
-    return -3;
+  const bool tcp = mixed::use_tc(np);
+  const size_t sm = tcp ? mixed::mixed_smem<true>(np) : mixed::mixed_smem<false>(np);
+  auto kernel = tcp ? mixed::rgf_mixed_kernel<true> : mixed::rgf_mixed_kernel<false>;
+  if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess) return -3;
   int nb = 0, dev = 0, nsm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, mixed::rgf_mixed_kernel, mixed::kThreads, sm) != cudaSuccess ||
-      nb <= 0)
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, mixed::kThreads, sm) != cudaSuccess || nb <= 0)
     return -3;
+  if (tcp && nb > 2) nb = 2;  // two blocks' TMEM per SM
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   return nb * nsm;
@@ -97,8 +128,13 @@ int rgf_mixed_grid(int np) {
 size_t rgf_mixed_ws_bytes(int np, int n, int grid) { return (size_t)grid * mixed::mixed_ws_bytes_per_block(np, n); }
 int rgf_mixed_launch(const RgfArgs& a, int np, int grid, void* ws, cudaStream_t st) {
   if (a.batch <= 0) return 0;
-  mixed::rgf_mixed_kernel<<<grid, mixed::kThreads, mixed::mixed_smem_bytes(np), st>>>(
-      a, np, static_cast<unsigned char*>(ws));
+  if (mixed::use_tc(np)) {
+    mixed::rgf_mixed_kernel<true><<<grid, mixed::kThreads, mixed::mixed_smem<true>(np), st>>>(
+        a, np, static_cast<unsigned char*>(ws));
+  } else {
+    mixed::rgf_mixed_kernel<false><<<grid, mixed::kThreads, mixed::mixed_smem<false>(np), st>>>(
+        a, np, static_cast<unsigned char*>(ws));
+  }
   return cudaGetLastError() == cudaSuccess ? 0 : -3;
 }
 

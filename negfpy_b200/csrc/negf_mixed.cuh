@@ -5,6 +5,7 @@
 #pragma once
 #include "negf_common.cuh"
 #include "negf_point.cuh"
+#include "negf_tcprod.cuh"
 #include "negf_tiles.cuh"
 
 namespace negf {
@@ -24,16 +25,6 @@ __device__ __forceinline__ float2 fmulc(float2 a, float2 b) {
 __device__ __forceinline__ float2 to_f(double2 v) { return make_float2((float)v.x, (float)v.y); }
 
 // ------------------------------------------------------ 3 x TF32 products --
-__device__ __forceinline__ unsigned tf32_rna(float x) {
-  unsigned r;
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-  return r;
-}
-// x = hi + lo with both parts representable in TF32.
-__device__ __forceinline__ void split_tf32(float x, unsigned& hi, unsigned& lo) {
-  hi = tf32_rna(x);
-  lo = tf32_rna(x - __uint_as_float(hi));
-}
 __device__ __forceinline__ void mma_tf32(float (&d)[4], const unsigned (&a)[4], unsigned b0, unsigned b1) {
   asm("mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
       : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
@@ -338,9 +329,12 @@ __host__ __device__ inline size_t mixed_ws_bytes_per_block(int np, int n) {
 // Sigma, Gamma and trace in FP64, the RGF sweep in FP32, for one point whose
 // blocks are selected in q.  `blk` is the block's workspace
 // (mixed_ws_bytes_per_block(NP, n) bytes).  Returns the status; *t the
-// transmission when kOk.
+// transmission when kOk.  TC: the sweep's four products per layer run on
+// tcgen05 (tc::cprod with the block's context *tcx; NP <= 128), otherwise on
+// mma.sync; the inversions run on mma.sync either way.
+template <bool TC = false>
 static __device__ int rgf_point_mixed(const glob::RgfPoint& q, int NP, unsigned char* blk, const GJS32& sh,
-                                      double* red, double* t) {
+                                      double* red, double* t, tc::Ctx* tcx = nullptr) {
   const int n = q.n, L = q.L, tid = threadIdx.x, warp = tid >> 5;
   const int np16 = NP >> 4, ntiles = np16 * np16, kch = (n + 7) >> 3;
   const long long M2 = (long long)NP * NP;
@@ -381,6 +375,33 @@ static __device__ int rgf_point_mixed(const glob::RgfPoint& q, int NP, unsigned 
     for (int l = 1; l < L && status == kOk; ++l) {
       load_pad32(pc, C + (long long)(l - 1) * q.c_ls, n, NP);
       __syncthreads();
+      const double2* Dl = D + (long long)l * q.d_ls;
+      const bool last = (l == L - 1);
+      if constexpr (TC) {
+        // W = g C, U = G_0 C, X = C^H W on tcgen05; M formed from X below
+        bool ok = tc::cprod<false, false>(bW, pg, pc, NP, *tcx);
+        ok = tc::cprod<false, false>(bU, bG0, pc, NP, *tcx) && ok;
+        ok = tc::cprod<true, false>(bX, pc, bW, NP, *tcx) && ok;
+        if (!ok) {
+          status = kNonFinite;
+          break;
+        }
+        for (long long e = tid; e < M2; e += kThreads) {
+          const int r = (int)(e / NP), cc = (int)(e - (long long)r * NP);
+          float2 v;
+          if (r < n && cc < n) {
+            double2 w = cneg(Dl[r * n + cc]);
+            if (last) w = csub(w, sigR[r * n + cc]);
+            if (r == cc) w = cadd(w, z);
+            const float2 x = bX[e];
+            v = make_float2((float)(w.x - (double)x.x), (float)(w.y - (double)x.y));
+          } else {
+            v = make_float2(r == cc ? 1.f : 0.f, 0.f);
+          }
+          pg[e] = v;
+        }
+        __syncthreads();
+      } else {
       // W = g_{l-1} C, U = G_{0,l-1} C
       for (int tt = warp; tt < ntiles; tt += kWarps) {
         const Tile T = tile_of(tt, np16);
@@ -399,8 +420,6 @@ static __device__ int rgf_point_mixed(const glob::RgfPoint& q, int NP, unsigned 
       __syncthreads();
       // M = z - D_l - C^H W [- Sigma_R on the last layer] into the old g buffer;
       // the FP64 terms are combined in FP64 before the rounding.
-      const double2* Dl = D + (long long)l * q.d_ls;
-      const bool last = (l == L - 1);
       for (int tt = warp; tt < ntiles; tt += kWarps) {
         const Tile T = tile_of(tt, np16);
         Acc32 c1;
@@ -423,6 +442,7 @@ static __device__ int rgf_point_mixed(const glob::RgfPoint& q, int NP, unsigned 
           }
       }
       __syncthreads();
+      }
       status = gj_invert32(pg, bX, n, NP, sh, &inv);
       if (status != kOk) break;
       if (inv != pg) {
@@ -430,16 +450,23 @@ static __device__ int rgf_point_mixed(const glob::RgfPoint& q, int NP, unsigned 
         pg = inv;
       }
       // G_{0,l} = U g_l
-      for (int tt = warp; tt < ntiles; tt += kWarps) {
-        const Tile T = tile_of(tt, np16);
-        Acc32 c1;
-        tile_mm32<false, false>(c1, bU, pg, NP, kch, T);
+      if constexpr (TC) {
+        if (!tc::cprod<false, false>(bG0, bU, pg, NP, *tcx)) {
+          status = kNonFinite;
+          break;
+        }
+      } else {
+        for (int tt = warp; tt < ntiles; tt += kWarps) {
+          const Tile T = tile_of(tt, np16);
+          Acc32 c1;
+          tile_mm32<false, false>(c1, bU, pg, NP, kch, T);
 #pragma unroll
-        for (int j = 0; j < 2; ++j)
+          for (int j = 0; j < 2; ++j)
 #pragma unroll
-          for (int qq = 0; qq < 4; ++qq) bG0[(long long)tr(T, qq) * NP + tc(T, j, qq)] = c1.get(j, qq);
+            for (int qq = 0; qq < 4; ++qq) bG0[(long long)tr(T, qq) * NP + tc(T, j, qq)] = c1.get(j, qq);
+        }
+        __syncthreads();
       }
-      __syncthreads();
     }
   }
   // FP64: Gamma_L, Gamma_R, G widened, T = Re sum (Gamma_L G Gamma_R)_ij conj(G_ij).

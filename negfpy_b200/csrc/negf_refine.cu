@@ -27,6 +27,7 @@
 #include "negf_common.cuh"
 #include "negf_f64.h"
 #include "negf_mixed.cuh"
+#include "negf_tcprod.cuh"
 #include "negf_tiles.cuh"
 
 namespace negf {
@@ -73,8 +74,33 @@ __device__ __forceinline__ void pad64(double2* dst, const double2* src, int n, i
   glob::load_pad(dst, src, n, n, NP, 0.0);
 }
 
+// dst = op(A) op(B) for padded NP x NP FP32 matrices: on tcgen05 (TC; the
+// block's context *tcx) or on 3 x TF32 mma.sync tiles (contraction over the
+// kch chunks of the logical order).  Ends with the block synchronised;
+// false if a tcgen05 completion wait ran out.
+template <bool TC, bool AC, bool BC>
+__device__ bool prod32(float2* dst, const float2* A, const float2* B, int NP, int kch, tc::Ctx* tcx) {
+  if constexpr (TC) {
+    return tc::cprod<AC, BC>(dst, A, B, NP, *tcx);
+  } else {
+    const int np16 = NP >> 4, ntiles = np16 * np16;
+    for (int tt = threadIdx.x >> 5; tt < ntiles; tt += kWarps) {
+      const Tile T = tile_of(tt, np16);
+      Acc32 c1;
+      tile_mm32<AC, BC>(c1, A, B, NP, kch, T);
+#pragma unroll
+      for (int j = 0; j < 2; ++j)
+#pragma unroll
+        for (int qq = 0; qq < 4; ++qq) dst[(long long)tr(T, qq) * NP + tc(T, j, qq)] = c1.get(j, qq);
+    }
+    __syncthreads();
+    return true;
+  }
+}
+
+template <bool TC>
 static __device__ int refine_point(const glob::RgfPoint& q, int NP, unsigned char* blk, const GJS32& sh,
-                                   double* red, double tol, int maxit, double* t, int* steps) {
+                                   double* red, double tol, int maxit, double* t, int* steps, tc::Ctx* tcx) {
   const int n = q.n, L = q.L, tid = threadIdx.x, warp = tid >> 5;
   const int np16 = NP >> 4, ntiles = np16 * np16, kch = (n + 7) >> 3;
   const long long M2 = (long long)NP * NP;
@@ -100,42 +126,30 @@ static __device__ int refine_point(const glob::RgfPoint& q, int NP, unsigned cha
     if (l > 0) {
       load_pad32(pc, Cl(l - 1), n, NP);
       __syncthreads();
-      for (int tt = warp; tt < ntiles; tt += kWarps) {  // tA = g_{l-1} C_{l-1}
-        const Tile T = tile_of(tt, np16);
-        Acc32 c1;
-        tile_mm32<false, false>(c1, gs + (l - 1) * M2, pc, NP, kch, T);
-#pragma unroll
-        for (int j = 0; j < 2; ++j)
-#pragma unroll
-          for (int qq = 0; qq < 4; ++qq) tA[(long long)tr(T, qq) * NP + tc(T, j, qq)] = c1.get(j, qq);
+      bool ok = prod32<TC, false, false>(tA, gs + (l - 1) * M2, pc, NP, kch, tcx);  // g_{l-1} C_{l-1}
+      ok = prod32<TC, true, false>(bX, pc, tA, NP, kch, tcx) && ok;                 // C^H g C
+      if (!ok) {
+        status = kNonFinite;
+        break;
       }
-      __syncthreads();
     }
-    // M_l = z - D_l [- Sigma_L] [- Sigma_R] - C^H tA; the FP64 terms are
+    // M_l = z - D_l [- Sigma_L] [- Sigma_R] - C^H g C; the FP64 terms are
     // combined in FP64 before the rounding.
     const double2* D = Dl(l);
-    for (int tt = warp; tt < ntiles; tt += kWarps) {
-      const Tile T = tile_of(tt, np16);
-      Acc32 c1;
-      if (l > 0) tile_mm32<true, false>(c1, pc, tA, NP, kch, T);
-      else c1.zero();
-#pragma unroll
-      for (int j = 0; j < 2; ++j)
-#pragma unroll
-        for (int qq = 0; qq < 4; ++qq) {
-          const int r = tr(T, qq), cc = tc(T, j, qq);
-          float2 v;
-          if (r < n && cc < n) {
-            double2 w = cneg(D[r * n + cc]);
-            if (l == 0) w = csub(w, sigL[r * n + cc]);
-            if (l == L - 1) w = csub(w, sigR[r * n + cc]);
-            if (r == cc) w = cadd(w, z);
-            v = make_float2((float)(w.x - (double)c1.re[j][qq]), (float)(w.y - (double)c1.im[j][qq]));
-          } else {
-            v = make_float2(r == cc ? 1.f : 0.f, 0.f);
-          }
-          bM[(long long)r * NP + cc] = v;
-        }
+    for (long long e = tid; e < M2; e += kThreads) {
+      const int r = (int)(e / NP), cc = (int)(e - (long long)r * NP);
+      float2 v;
+      if (r < n && cc < n) {
+        double2 w = cneg(D[r * n + cc]);
+        if (l == 0) w = csub(w, sigL[r * n + cc]);
+        if (l == L - 1) w = csub(w, sigR[r * n + cc]);
+        if (r == cc) w = cadd(w, z);
+        const float2 x = l > 0 ? bX[e] : make_float2(0.f, 0.f);
+        v = make_float2((float)(w.x - (double)x.x), (float)(w.y - (double)x.y));
+      } else {
+        v = make_float2(r == cc ? 1.f : 0.f, 0.f);
+      }
+      bM[e] = v;
     }
     __syncthreads();
     float2* inv = nullptr;
@@ -153,34 +167,13 @@ static __device__ int refine_point(const glob::RgfPoint& q, int NP, unsigned cha
   copy32(tA, gs + (L - 1) * M2, NP);
   widen_pad(X64 + (L - 1) * M2, gs + (L - 1) * M2, n, NP);
   __syncthreads();
-  for (int i = L - 2; i >= 0; --i) {
+  for (int i = L - 2; i >= 0 && status == kOk; --i) {
     load_pad32(pc, Cl(i), n, NP);
     __syncthreads();
-    for (int tt = warp; tt < ntiles; tt += kWarps) {  // tB = C_i X_{i+1}
-      const Tile T = tile_of(tt, np16);
-      Acc32 c1;
-      tile_mm32<false, false>(c1, pc, tA, NP, kch, T);
-#pragma unroll
-      for (int j = 0; j < 2; ++j)
-#pragma unroll
-        for (int qq = 0; qq < 4; ++qq) tB[(long long)tr(T, qq) * NP + tc(T, j, qq)] = c1.get(j, qq);
-    }
-    __syncthreads();
-    for (int tt = warp; tt < ntiles; tt += kWarps) {  // X_i = g_i tB
-      const Tile T = tile_of(tt, np16);
-      Acc32 c1;
-      tile_mm32<false, false>(c1, gs + i * M2, tB, NP, kch, T);
-#pragma unroll
-      for (int j = 0; j < 2; ++j)
-#pragma unroll
-        for (int qq = 0; qq < 4; ++qq) {
-          const int r = tr(T, qq), cc = tc(T, j, qq);
-          const float2 v = c1.get(j, qq);
-          tA[(long long)r * NP + cc] = v;
-          X64[i * M2 + (long long)r * NP + cc] =
-              (r < n && cc < n) ? make_double2((double)v.x, (double)v.y) : make_double2(0.0, 0.0);
-        }
-    }
+    bool ok = prod32<TC, false, false>(tB, pc, tA, NP, kch, tcx);           // C_i X_{i+1}
+    ok = prod32<TC, false, false>(tA, gs + i * M2, tB, NP, kch, tcx) && ok;  // X_i = g_i C_i X_{i+1}
+    if (!ok) status = kNonFinite;
+    widen_pad(X64 + i * M2, tA, n, NP);
     __syncthreads();
   }
   // Sigma_L and Sigma_R padded for the residual products.
@@ -191,10 +184,10 @@ static __device__ int refine_point(const glob::RgfPoint& q, int NP, unsigned cha
   // 3. Refinement.
   double nu_prev = 0.0;
   bool done = false;
-  for (int it = 1; it <= maxit && !done; ++it) {
+  for (int it = 1; it <= maxit && !done && status == kOk; ++it) {
     *steps = it;
     // forward: R_i in FP64, t_i = R_i + C_{i-1}^H y_{i-1}, y_i = g_i t_i
-    for (int i = 0; i < L; ++i) {
+    for (int i = 0; i < L && status == kOk; ++i) {
       pad64(Dp, Dl(i), n, NP);
       if (i > 0) {
         pad64(Cm, Cl(i - 1), n, NP);
@@ -202,6 +195,10 @@ static __device__ int refine_point(const glob::RgfPoint& q, int NP, unsigned cha
       }
       if (i < L - 1) pad64(Cn, Cl(i), n, NP);
       __syncthreads();
+      if (i > 0 && !prod32<TC, true, false>(bM, pc, ys + (i - 1) * M2, NP, kch, tcx)) {
+        status = kNonFinite;
+        break;
+      }
       const double2* Xi = X64 + i * M2;
       for (int tt = warp; tt < ntiles; tt += kWarps) {
         const Tile T = tile_of(tt, np16);
@@ -211,37 +208,27 @@ static __device__ int refine_point(const glob::RgfPoint& q, int NP, unsigned cha
         if (i < L - 1) tile_mm<false, false, true>(a, Cn, NP, Xi + M2, NP, kch, T);
         if (i == 0) tile_mm<false, false, true>(a, B0, NP, Xi, NP, kch, T);
         if (i == L - 1) tile_mm<false, false, true>(a, B1, NP, Xi, NP, kch, T);
-        Acc32 c1;
-        if (i > 0) tile_mm32<true, false>(c1, pc, ys + (i - 1) * M2, NP, kch, T);
-        else c1.zero();
 #pragma unroll
         for (int j = 0; j < 2; ++j)
 #pragma unroll
           for (int qq = 0; qq < 4; ++qq) {
             const int r = tr(T, qq), cc = tc(T, j, qq);
+            const long long e = (long long)r * NP + cc;
             float2 v = make_float2(0.f, 0.f);
             if (r < n && cc < n) {
-              const double2 x = Xi[(long long)r * NP + cc];
               // R = E - (z X - D X - C^H X - C X - Sigma X)
-              double2 rv = csub(a.get(j, qq), cmul(z, x));
+              double2 rv = csub(a.get(j, qq), cmul(z, Xi[e]));
               if (i == L - 1 && r == cc) rv.x += 1.0;
-              v = make_float2((float)rv.x + c1.re[j][qq], (float)rv.y + c1.im[j][qq]);
+              const float2 cy = i > 0 ? bM[e] : make_float2(0.f, 0.f);
+              v = make_float2((float)rv.x + cy.x, (float)rv.y + cy.y);
             }
-            tA[(long long)r * NP + cc] = v;
+            tA[e] = v;
           }
       }
       __syncthreads();
-      for (int tt = warp; tt < ntiles; tt += kWarps) {  // y_i = g_i t_i
-        const Tile T = tile_of(tt, np16);
-        Acc32 c1;
-        tile_mm32<false, false>(c1, gs + i * M2, tA, NP, kch, T);
-#pragma unroll
-        for (int j = 0; j < 2; ++j)
-#pragma unroll
-          for (int qq = 0; qq < 4; ++qq) ys[i * M2 + (long long)tr(T, qq) * NP + tc(T, j, qq)] = c1.get(j, qq);
-      }
-      __syncthreads();
+      if (!prod32<TC, false, false>(ys + i * M2, gs + i * M2, tA, NP, kch, tcx)) status = kNonFinite;  // y_i
     }
+    if (status != kOk) break;
     // backward: d_{L-1} = y_{L-1}, d_i = y_i + g_i C_i d_{i+1}; X += d
     double dmax = 0.0, xmax = 0.0;
     for (int i = L - 1; i >= 0; --i) {
@@ -250,41 +237,29 @@ static __device__ int refine_point(const glob::RgfPoint& q, int NP, unsigned cha
       if (i < L - 1) {
         load_pad32(pc, Cl(i), n, NP);
         __syncthreads();
-        for (int tt = warp; tt < ntiles; tt += kWarps) {  // tB = C_i d_{i+1}
-          const Tile T = tile_of(tt, np16);
-          Acc32 c1;
-          tile_mm32<false, false>(c1, pc, yi + M2, NP, kch, T);
-#pragma unroll
-          for (int j = 0; j < 2; ++j)
-#pragma unroll
-            for (int qq = 0; qq < 4; ++qq) tB[(long long)tr(T, qq) * NP + tc(T, j, qq)] = c1.get(j, qq);
+        bool ok = prod32<TC, false, false>(tB, pc, yi + M2, NP, kch, tcx);        // C_i d_{i+1}
+        ok = prod32<TC, false, false>(bM, gs + i * M2, tB, NP, kch, tcx) && ok;  // g_i C_i d_{i+1}
+        if (!ok) {
+          status = kNonFinite;
+          break;
         }
-        __syncthreads();
       }
-      for (int tt = warp; tt < ntiles; tt += kWarps) {
-        const Tile T = tile_of(tt, np16);
-        Acc32 c1;
-        if (i < L - 1) tile_mm32<false, false>(c1, gs + i * M2, tB, NP, kch, T);
-        else c1.zero();
-#pragma unroll
-        for (int j = 0; j < 2; ++j)
-#pragma unroll
-          for (int qq = 0; qq < 4; ++qq) {
-            const int r = tr(T, qq), cc = tc(T, j, qq);
-            const long long e = (long long)r * NP + cc;
-            const float2 y = yi[e];
-            const float2 d = make_float2(__fadd_rn(y.x, c1.re[j][qq]), __fadd_rn(y.y, c1.im[j][qq]));
-            yi[e] = d;
-            if (r < n && cc < n) {
-              const double2 x = cadd(Xi[e], make_double2((double)d.x, (double)d.y));
-              Xi[e] = x;
-              dmax = fmax(dmax, fmax(fabs((double)d.x), fabs((double)d.y)));
-              xmax = fmax(xmax, fmax(fabs(x.x), fabs(x.y)));
-            }
-          }
+      for (long long e = tid; e < M2; e += kThreads) {
+        const int r = (int)(e / NP), cc = (int)(e - (long long)r * NP);
+        const float2 y = yi[e];
+        const float2 c1 = i < L - 1 ? bM[e] : make_float2(0.f, 0.f);
+        const float2 d = make_float2(__fadd_rn(y.x, c1.x), __fadd_rn(y.y, c1.y));
+        yi[e] = d;
+        if (r < n && cc < n) {
+          const double2 x = cadd(Xi[e], make_double2((double)d.x, (double)d.y));
+          Xi[e] = x;
+          dmax = fmax(dmax, fmax(fabs((double)d.x), fabs((double)d.y)));
+          xmax = fmax(xmax, fmax(fabs(x.x), fabs(x.y)));
+        }
       }
       __syncthreads();
     }
+    if (status != kOk) break;
     int bad = !(isfinite(dmax) && isfinite(xmax));
     if (block_any(bad)) {
       status = kNonFinite;
@@ -318,14 +293,32 @@ static __device__ int refine_point(const glob::RgfPoint& q, int NP, unsigned cha
   return status;
 }
 
+// Dynamic shared memory: [tcgen05 stage and mbarrier (TC only) | GJ panel,
+// pivot bookkeeping | reduction scratch].  With TC at least 80 KB, so that at
+// most two blocks share an SM and their TMEM (2 x 256 columns) always fits.
+__host__ __device__ inline size_t tc_bytes(int np) { return ((tc::stage_bytes(np) + 16 + 127) / 128) * 128; }
+template <bool TC>
+size_t smem_bytes(int np) {
+  const size_t base = ((mixed::gjs32_bytes(np) + 15) / 16) * 16 + 40 * 8;
+  if (!TC) return base;
+  const size_t need = tc_bytes(np) + base;
+  return need > 80 * 1024 ? need : 80 * 1024;
+}
+
+template <bool TC>
 __global__ void __launch_bounds__(kThreads, 2) rgf_refine_kernel(RgfArgs a, int NP, unsigned char* ws, double tol,
                                                                  int maxit, int* steps_out) {
-  extern __shared__ __align__(16) unsigned char smraw[];
-  const GJS32 sh = mixed::carve32(smraw, NP);
-  double* red = reinterpret_cast<double*>(smraw + ((mixed::gjs32_bytes(NP) + 15) / 16) * 16);
+  extern __shared__ __align__(128) unsigned char smraw[];
+  unsigned char* gj = smraw + (TC ? tc_bytes(NP) : 0);
+  const GJS32 sh = mixed::carve32(gj, NP);
+  double* red = reinterpret_cast<double*>(gj + ((mixed::gjs32_bytes(NP) + 15) / 16) * 16);
   __shared__ int s_point;
+  __shared__ uint32_t s_tmem;
+  __shared__ int s_tcerr;
   const int n = a.n, tid = threadIdx.x;
   unsigned char* blk = ws + (long long)blockIdx.x * ws_bytes_per_block(NP, n, a.L);
+  tc::Ctx tcx;
+  if constexpr (TC) tcx = tc::setup(smraw, NP, &s_tmem, &s_tcerr);
 
   for (;;) {
     if (tid == 0) s_point = (int)atomicAdd(a.counter, 1u);
@@ -359,7 +352,7 @@ __global__ void __launch_bounds__(kThreads, 2) rgf_refine_kernel(RgfArgs a, int 
     q.z = glob::z_of(a.omega[p], a.eta_dev[p]);
     double tval = 0.0;
     int steps = 0;
-    const int status = refine_point(q, NP, blk, sh, red, tol, maxit, &tval, &steps);
+    const int status = refine_point<TC>(q, NP, blk, sh, red, tol, maxit, &tval, &steps, &tcx);
     if (tid == 0) {
       a.T_out[p] = (status == kOk) ? tval : __longlong_as_double(0x7ff8000000000000ULL);
       if (a.status_out) a.status_out[p] = status;
@@ -367,25 +360,24 @@ __global__ void __launch_bounds__(kThreads, 2) rgf_refine_kernel(RgfArgs a, int 
     }
     __syncthreads();
   }
+  if constexpr (TC) tc::teardown(tcx);
 }
-
-size_t smem_bytes(int np) { return ((mixed::gjs32_bytes(np) + 15) / 16) * 16 + 40 * 8; }
 
 }  // namespace refine
 
+bool refine_use_tc(int np) { return mixed::use_tc(np); }
+
 int rgf_refine_grid(int np) {
-  const size_t sm = refine::smem_bytes(np);
-  if (cudaFuncSetAttribute(refine::rgf_refine_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) !=
-      cudaSuccess)
-    return -3;
+  const bool tcp = refine_use_tc(np);
+  const size_t sm = tcp ? refine::smem_bytes<true>(np) : refine::smem_bytes<false>(np);
+  auto kernel = tcp ? refine::rgf_refine_kernel<true> : refine::rgf_refine_kernel<false>;
+  if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess) return -3;
   int nb = 0, dev = 0, nsm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, refine::rgf_refine_kernel, refine::kThreads, sm) !=
-          cudaSuccess ||
-      nb <= 0)
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, refine::kThreads, sm) != cudaSuccess || nb <= 0)
     return -3;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-  if (nb > 2) nb = 2;  // the L-slot workspace grows with the grid
+  if (nb > 2) nb = 2;  // the L-slot workspace grows with the grid; two blocks' TMEM per SM
   return nb * nsm;
 }
 size_t rgf_refine_ws_bytes(int np, int n, int L, int grid) {
@@ -394,8 +386,13 @@ size_t rgf_refine_ws_bytes(int np, int n, int L, int grid) {
 int rgf_refine_launch(const RgfArgs& a, int np, int grid, void* ws, double tol, int maxit, int* steps_out,
                       cudaStream_t st) {
   if (a.batch <= 0) return 0;
-  refine::rgf_refine_kernel<<<grid, refine::kThreads, refine::smem_bytes(np), st>>>(
-      a, np, static_cast<unsigned char*>(ws), tol, maxit, steps_out);
+  if (refine_use_tc(np)) {
+    refine::rgf_refine_kernel<true><<<grid, refine::kThreads, refine::smem_bytes<true>(np), st>>>(
+        a, np, static_cast<unsigned char*>(ws), tol, maxit, steps_out);
+  } else {
+    refine::rgf_refine_kernel<false><<<grid, refine::kThreads, refine::smem_bytes<false>(np), st>>>(
+        a, np, static_cast<unsigned char*>(ws), tol, maxit, steps_out);
+  }
   return cudaGetLastError() == cudaSuccess ? 0 : -3;
 }
 

@@ -498,3 +498,20 @@ class StackedSystem:
             itr[sl] = rr["iters"]
         return {"T": T, "status": st, "iters_left": itl, "iters_right": itr, "fallback": n_fallback,
                 "steps": steps_all}
+
+
+def cgemm_tf32x3(a: torch.Tensor, b: torch.Tensor, conj_a: bool = False, conj_b: bool = False,
+                 stream=None) -> tuple[torch.Tensor, torch.Tensor]:
+    """op(a) @ op(b) for batches of complex64 n x n matrices ``[P, n, n]`` on
+    tcgen05 tensor cores (3 x TF32 split, ``negf_cgemm_tf32x3``); returns the
+    products and a per-product status."""
+    lib = _lib.load()
+    dev = _dev()
+    a = a.to(device=dev, dtype=torch.complex64).contiguous()
+    b = b.to(device=dev, dtype=torch.complex64).contiguous()
+    P, n, _ = a.shape
+    c = torch.empty_like(a)
+    st = torch.full((P,), -1, dtype=torch.int32, device=dev)
+    _lib.check(lib.negf_cgemm_tf32x3(n, P, _lib.ptr(a), _lib.ptr(b), _lib.ptr(c), int(conj_a), int(conj_b),
+                                     _lib.ptr(st), _lib.stream_handle(stream)), "negf_cgemm_tf32x3")
+    return c, st

@@ -195,13 +195,17 @@ def test_hetero_lead_grads_match_central_differences(hetero):
     """Central differences of the forward kernels (leads rebuilt and decimated
     again at every evaluation) on 50 lead parameters and 10 shared masses.
 
-    Near band edges the decimated T moves by ~1e-7 relative under 1e-16
-    changes of the lead blocks (negfpy's algorithm does the same), so each
-    kappa evaluation carries ~1e-10 relative noise and a difference quotient
-    with h = 1e-6 carries up to ~1e-4 of it; a larger h does not help, since
-    the lead parameters move band edges across the omega grid and kappa on
-    the grid is only piecewise smooth in them.  Bound: 2e-4 of the largest
-    gradient component at every parameter, 1e-6 at the median."""
+    The lead parameters move band edges across the omega grid, so kappa on
+    the grid is smooth in them only on a small scale: a step-size study
+    (h = 1e-7 ... 1e-3 on six parameters) shows the difference quotient
+    approaching the adjoint value as h falls to 1e-6, with truncation error
+    growing as h^2 above it (2e-4 of the largest component at h = 1e-5,
+    2e-3 at 1e-4) and rounding noise of the decimation near band edges
+    growing below it.  At h = 1e-6 both are a few 1e-15 W/K per unit
+    parameter, ~5e-6 of kappa, whatever the size of the component.  Bound:
+    |FD - adjoint| <= 2e-5 kappa at every parameter and 5e-6 kappa at the
+    median.  (Spring constants of the device alone agree to 1e-10 relative
+    with the same h.)"""
     m = hetero.model
     assert m.n == 72 and m.n_a == 48 and m.L == 30
     th, ms, pa, pb = _params(hetero)
@@ -227,9 +231,10 @@ def test_hetero_lead_grads_match_central_differences(hetero):
         args_p[pos], args_m[pos] = xp.reshape(args_p[pos].shape), xm.reshape(args_m[pos].shape)
         return (hetero.kappa_full(*args_p) - hetero.kappa_full(*args_m)) / (2 * h)
 
+    k = abs(float(kap))
     for which, sel, grad in (("a", sel_a, d_pa), ("b", sel_b, d_pb), ("m", msel, d_m)):
         ga = grad.reshape(-1).cpu().numpy()
-        scale = np.abs(ga).max()
-        err = np.abs(np.array([fd(which, q, 1e-6) for q in sel]) - ga[sel]) / scale
-        assert float(err.max()) < 2e-4 and float(np.median(err)) < 1e-6, (which, float(err.max()),
+        assert np.abs(ga[sel]).max() > 1e-3 * k
+        err = np.abs(np.array([fd(which, q, 1e-6) for q in sel]) - ga[sel]) / k
+        assert float(err.max()) < 2e-5 and float(np.median(err)) < 5e-6, (which, float(err.max()),
                                                                           float(np.median(err)))

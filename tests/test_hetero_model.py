@@ -104,3 +104,41 @@ def test_kappa_weights_trapezoid():
     fine = torch.linspace(0.01, 3.0, 300001, dtype=torch.float64)
     wf = kappa_weights(fine, 300.0, 1e13)
     assert abs(float(w.sum() / wf.sum()) - 1) < 1e-4
+
+
+def test_material_tables_default_to_the_model_and_build_the_leads():
+    """The material spring tables reproduce the model's bonds and leads at
+    their defaults; the torch lead builder equals the numpy one; equal
+    parameters give bitwise-equal blocks."""
+    m = HeteroModel(seed=7, ny=2, nz_a=2, nz_b=4, n_layers=6, n_params=60)
+    th = torch.as_tensor(m.theta0, dtype=torch.float64)
+    pa, pb = torch.as_tensor(m.phi0_a), torch.as_tensor(m.phi0_b)
+    assert torch.equal(m.spring_values(th), m.spring_values(th, pa, pb))
+    on0, cp0 = m.blocks(th, KP)
+    on1, cp1 = m.blocks(th, KP, phi_a=pa, phi_b=pb)
+    assert torch.equal(on0, on1) and torch.equal(cp0, cp1)
+    for mat, phi in (("A", pa), ("B", pb)):
+        ref = m.lead_blocks(mat, KP)
+        got = m.lead_blocks_torch(mat, KP, phi)
+        for key in ("d00", "d01", "d10"):
+            assert np.abs(got[key].resolve_conj().numpy() - ref[key]).max() < 1e-14
+        again = m.lead_blocks_torch(mat, KP, phi)
+        assert torch.equal(got["d00"], again["d00"]) and torch.equal(got["d01"], again["d01"])
+
+
+def test_material_table_reaches_lead_and_device():
+    """A material-table entry moves the lead blocks and the device bonds of
+    that material (a parameter shared by lead and device); theta overrides
+    the bonds it owns."""
+    m = HeteroModel(seed=7, ny=2, nz_a=2, nz_b=4, n_layers=6, n_params=60)
+    th = torch.as_tensor(m.theta0, dtype=torch.float64)
+    src, key = m.bond_src, m.bond_key
+    free = [b for b in np.flatnonzero(src == 1) if not m.is_param[b]]
+    q = int(key[free[0]])
+    pa = torch.as_tensor(m.phi0_a).clone()
+    pa[q] += 0.25
+    kv0, kv1 = m.spring_values(th), m.spring_values(th, phi_a=pa)
+    moved = np.flatnonzero((kv1 - kv0).abs().numpy() > 0)
+    assert set(moved) == {b for b in np.flatnonzero((src == 1) & (key == q)) if not m.is_param[b]}
+    la0, la1 = m.lead_blocks_torch("A", KP), m.lead_blocks_torch("A", KP, pa)
+    assert float((la1["d00"] - la0["d00"]).abs().max()) > 0
