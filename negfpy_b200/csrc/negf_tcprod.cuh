@@ -15,7 +15,8 @@
 // the instruction descriptor.  K runs in slabs of KS = 16: the block stages
 // a slab of both operands in shared memory (split and laid out in the
 // no-swizzle K-major core-matrix layout), one thread issues the slab's 24
-// MMAs and commits them to an mbarrier, every thread waits on it (bounded),
+// MMAs and commits them to an mbarrier, every thread waits on it (at most
+// 2 s of wall time; then the product reports failure),
 // and the next slab is staged.  The result is read back with tcgen05.ld and
 // written to C.
 #pragma once
@@ -31,7 +32,7 @@ constexpr int KS = 16;               // K per staged slab: two MMA steps of 8
 constexpr int MT = 128;              // MMA tile rows (M)
 constexpr int kMaxNP = 128;
 constexpr int kTmemCols = 256;       // 2 kMaxNP FP32 columns
-constexpr uint32_t kWaitLimit = 1u << 26;
+constexpr uint64_t kWaitLimitNs = 2000000000ull;  // 2 s per slab: far above any real completion time
 
 // Shared memory of the product: 4 A parts (128 x KS) and 4 B parts (NP x KS).
 __host__ __device__ constexpr size_t stage_bytes(int np) { return (size_t)4 * MT * KS * 4 + (size_t)4 * np * KS * 4; }
@@ -123,7 +124,7 @@ __device__ bool cprod(float2* __restrict__ C, const float2* __restrict__ A, cons
       umma::mma_commit(ctx.bar);
     }
     if (ok) {
-      ok = umma::mbar_wait(ctx.bar, ctx.phase, kWaitLimit);
+      ok = umma::mbar_wait(ctx.bar, ctx.phase, kWaitLimitNs);
       ctx.phase ^= 1u;
     }
     if (!ok && lane == 0) *ctx.err = 1;

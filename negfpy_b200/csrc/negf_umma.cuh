@@ -41,22 +41,30 @@ __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.
 __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
 }
-// Waits for the phase with the given parity to complete; gives up after
-// `limit` polls and returns false (the caller reports the failure).
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32_t limit) {
+__device__ __forceinline__ uint64_t globaltimer_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+  return t;
+}
+// Waits for the phase with the given parity to complete, polling with the
+// non-blocking test_wait; gives up after `limit_ns` nanoseconds of wall time
+// and returns false (the caller reports the failure).
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint64_t limit_ns) {
   const uint32_t a = smem_u32(bar);
-  for (uint32_t i = 0; i < limit; ++i) {
+  const uint64_t t0 = globaltimer_ns();
+  for (;;) {
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
         "selp.u32 %0, 1, 0, p;\n\t}"
         : "=r"(done)
         : "r"(a), "r"(parity)
         : "memory");
     if (done) return true;
+    if (globaltimer_ns() - t0 > limit_ns) return false;
+    __nanosleep(20);
   }
-  return false;
 }
 // The mbarrier receives one arrival when every tcgen05.mma issued so far by
 // this thread has completed.
