@@ -426,7 +426,7 @@ def grad_vs_forward(torch, n_k=8, n_omega=256, reps=3):
                                    "differentiation through the sweeps) + autograd through the block builders"}}
 
 
-def uneven_batch(torch, omega_stride=16):
+def uneven_batch(torch, omega_stride=16, oracle_per_system=2):
     """The uneven batch (64 seeded systems, n in {24..192}, 10-60 layers,
     1-256 k, 1024 omegas each) on every ``omega_stride``-th omega of each
     system: autotuned launch shape and item order, one persistent launch per
@@ -489,11 +489,45 @@ def uneven_batch(torch, omega_stride=16):
         k64 = float((wk * a).sum())
         errs.append((float((wk * m).sum()) - k64) / k64)
     errs = np.abs(np.array(errs))
+    # Every system against the oracle (negfpy's algorithm) at sampled points.
+    from oracle import negf_oracle as O
+
+    rng = np.random.default_rng(17)
+    pairs, where = [], []
+    for i, w in enumerate(ws):
+        K = len(w.kpoints)
+        for _ in range(oracle_per_system):
+            wi, ki = int(rng.integers(0, oms[i].size)), int(rng.integers(0, K))
+            pairs.append((i, int(np.flatnonzero(w.omegas == oms[i][wi])[0]), ki))
+            where.append(int(offs[i]) + wi * K + ki)
+    cores = os.cpu_count() or 1
+    pool = O.make_pool(cores)
+    try:
+        t0 = time.perf_counter()
+        args = [O.workload_point_args(ws[i], wi, ki) for i, wi, ki in pairs]
+        t_or = np.array(pool.map(O._pool_task, args, chunksize=1))
+        dt = time.perf_counter() - t0
+    finally:
+        pool.close()
+        pool.join()
+    sel = torch.as_tensor(where, device="cuda")
+    rel = {p: np.abs(res[p][sel].cpu().numpy() - t_or) / np.maximum(np.abs(t_or), 1.0) for p in ("f64", "mixed")}
+    per_sys = {p: [float(np.nanmax(rel[p][j * oracle_per_system:(j + 1) * oracle_per_system]))
+                   for j in range(len(ws))] for p in rel}
+    oracle = {"points": len(pairs), "per_system": oracle_per_system, "seconds": dt, "cores": cores,
+              "f64_T_rel_err_max": float(np.nanmax(rel["f64"])),
+              "f64_T_rel_err_median": float(np.nanmedian(rel["f64"])),
+              "f64_points_above_1e-10": int((rel["f64"] > 1e-10).sum()),
+              "mixed_T_rel_err_max": float(np.nanmax(rel["mixed"])),
+              "mixed_T_rel_err_median": float(np.nanmedian(rel["mixed"])),
+              "per_system_max": per_sys}
     return {"workload": f"64 systems, n in {{24..192}}, L 10-60, K 1-256, every {omega_stride}th of 1024 omegas "
                         f"({int(offs[-1])} points)",
             "f64": out["f64"], "mixed": out["mixed"],
             "speedup": out["mixed"]["points_per_s"] / out["f64"]["points_per_s"],
             "kappa_rel_err_max": float(errs.max()), "kappa_rel_err_median": float(np.median(errs)),
+            "kappa_err_reference": "the FP64 batch on the same omegas (kappa needs the whole omega grid)",
+            "oracle_sample": oracle,
             "launch": "one persistent kernel per solve, replayed from a CUDA graph; shape and order autotuned"}
 
 

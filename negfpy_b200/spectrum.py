@@ -80,10 +80,15 @@ def grid_points(W: int, K: int, device=None):
 def transmission_grid(omegas, kpoints, device, lead_left, lead_right, eta: float = 1e-8,
                       eta_device: float | None = None, device_to_lead_left=None, device_to_lead_right=None,
                       contact_left_indices=None, contact_right_indices=None, surface_gf_method: str = "sancho_rubio",
-                      omega_scale: float | None = None, tol: float = 1e-12, maxiter: int = 200) -> dict:
+                      omega_scale: float | None = None, tol: float = 1e-12, maxiter: int = 200,
+                      precision: str = "f64") -> dict:
     """T[w, k] for every omega and k (numpy arrays ``T``, ``status``, ``iters_left``, ``iters_right``).
 
     Each entry equals ``negfpy.core.transmission(omegas[w], ..., kpar=kpoints[k])``.
+    ``precision``: "f64"; "refined" (FP32 factors of the device solve refined
+    to FP64 accuracy, FP64 re-solve of the points that fail; adds ``steps``
+    and the count ``fallback``); "mixed" (unrefined FP32 sweep, about FP32
+    accuracy; adds ``fallback``).
     """
     check_method(surface_gf_method)
     dev = _lib.require_cuda()
@@ -99,8 +104,12 @@ def transmission_grid(omegas, kpoints, device, lead_left, lead_right, eta: float
     om_t = torch.tensor(om / s, dtype=torch.float64, device=dev)[w_idx]
     P = om.size * K
     r = sysobj.transmission(om_t, k_idx, torch.full((P,), eta / s, dtype=torch.float64, device=dev),
-                            torch.full((P,), eta_dev / s, dtype=torch.float64, device=dev), tol, maxiter)
-    return {key: v.reshape(om.size, K).cpu().numpy() for key, v in r.items() if torch.is_tensor(v)}
+                            torch.full((P,), eta_dev / s, dtype=torch.float64, device=dev), tol, maxiter,
+                            precision=precision)
+    out = {key: v.reshape(om.size, K).cpu().numpy() for key, v in r.items() if torch.is_tensor(v)}
+    if precision != "f64":
+        out["fallback"] = int(r["fallback"])
+    return out
 
 
 def kappa_from_grid(omegas, T_wk, temperatures, omega_unit_rad_s: float) -> np.ndarray:

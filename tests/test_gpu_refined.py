@@ -128,3 +128,23 @@ def test_stacked_system_precisions():
     assert rr["fallback"] == 0 and int(rr["steps"].min()) >= 1
     err = float(((rr["T"] - r64["T"]).abs() / r64["T"].abs().clamp_min(1.0)).max())
     assert err <= TOL, err
+
+
+def test_transmission_grid_precisions():
+    """The public grid call takes the precision: "refined" equals FP64 within
+    the parity bound; "mixed" within the FP32 sweep's error."""
+    import negfpy_b200 as nb
+    from negfpy_b200.models import material_kspace_device, material_kspace_lead
+
+    wl = W.slab_workload(n_omega=64, n_k=8, n_layers=6)
+    params = W.spring_network(wl.meta["seed"], ny=wl.meta["ny"], nz=wl.meta["nz"], periodic_y=True)
+    lead = material_kspace_lead(params)
+    dev = material_kspace_device(6, params)
+    om = wl.omegas[3::8]
+    r64 = nb.transmission_grid(om, wl.kpoints, dev, lead, lead, eta=wl.eta)
+    rr = nb.transmission_grid(om, wl.kpoints, dev, lead, lead, eta=wl.eta, precision="refined")
+    rm = nb.transmission_grid(om, wl.kpoints, dev, lead, lead, eta=wl.eta, precision="mixed")
+    assert rr["fallback"] == 0 and rr["steps"].min() >= 1
+    scale = np.maximum(np.abs(r64["T"]), 1.0)
+    assert (np.abs(rr["T"] - r64["T"]) / scale).max() <= TOL
+    assert (np.abs(rm["T"] - r64["T"]) / scale).max() <= 1e-4
