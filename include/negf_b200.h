@@ -225,6 +225,17 @@ int negf_rgf_transmission_refined(int n_dev, int n_lead_l, int n_lead_r, int n_l
 int negf_cgemm_tf32x3(int n, int batch, const float* a, const float* b, float* c, int conj_a, int conj_b,
                       int* status_out, void* stream);
 
+/*
+ * Product tiling of the FP32 device sweeps (negf_rgf_transmission_mixed,
+ * negf_rgf_transmission_refined) for block order n (padded to 16): path 0
+ * mma.sync 16 x 16 warp tiles, 1 tcgen05 128 x n tiles (n <= 128, else
+ * NEGF_EUNSUPPORTED), -1 back to the default (mma.sync unless NEGF_TC=1 in
+ * the environment).  Process-wide; returns the path now in effect (0 or 1).
+ * Set it before querying the workspace of the call it is meant for.  No
+ * counterpart in negfpy: the autotuner's switch (negfpy_b200.autotune).
+ */
+int negf_set_fp32_product_path(int n, int path);
+
 /* Workspace bytes negf_rgf_adjoint_f64 needs (0 on a bad size). */
 size_t negf_adjoint_workspace_bytes(int n_dev, int n_lead_l, int n_lead_r, int n_layers);
 

@@ -57,6 +57,7 @@ _SIGNATURES = {
          _I, _P, _P, _P, _P, _SZ, _P],
     ),
     "negf_cgemm_tf32x3": (_I, [_I, _I, _P, _P, _P, _I, _I, _P, _P]),
+    "negf_set_fp32_product_path": (_I, [_I, _I]),
     "negf_batch_max_grid": (_I, [_I, _I, _I]),
     "negf_batch_workspace_bytes": (_SZ, [_I, _I, _I, _I]),
     "negf_batch_system_bytes": (_SZ, []),

@@ -11,6 +11,13 @@ CUDA events, keeps the fastest, and caches the choice in a JSON file keyed by
 the GPU, the precision and the shape of the batch (block orders, layer counts
 and k counts of its systems).
 
+The FP32 device sweeps (mixed and refined precision) have two product
+tilings for block orders up to 128: 16 x 16 warp tiles on mma.sync, or
+128 x n tiles on the tcgen05 tensor cores with TMEM accumulators.
+``ProductPathTuner`` times both on a sample of a system's points and sets
+the faster one for that order (``negf_set_fp32_product_path``), cached the
+same way.
+
 Cache file: ``$NEGF_B200_TUNE_CACHE``, else ``~/.cache/negfpy_b200/autotune.json``.
 """
 
@@ -108,3 +115,44 @@ class BatchTuner:
             return best
 
         return self.select(key, measure, force)
+
+
+class ProductPathTuner(BatchTuner):
+    """Chooses the FP32 product tiling (0 mma.sync, 1 tcgen05) per block order."""
+
+    def __init__(self, cache_path: str | Path | None = None):
+        super().__init__(cache_path, candidates=[(1, "mma.sync"), (1, "tcgen05")])
+
+    def tune(self, system, omega, k_index, eta, precision: str = "mixed", reps: int = 2,
+             force: bool = False) -> dict:
+        """Times ``system.transmission(omega, k_index, eta, precision)`` with each
+        tiling, keeps the faster for ``system.n`` and returns the entry
+        (``path`` 0 or 1).  Orders above 128 have only mma.sync."""
+        import torch
+
+        from . import engine
+
+        n = system.n
+        if n > 128:
+            engine.set_fp32_product_path(n, 0)
+            return {"path": 0, "order": "mma.sync", "cached": False, "timings": {}}
+        gpu = torch.cuda.get_device_name() + f"/{torch.cuda.get_device_properties(0).multi_processor_count}SM"
+        key = batch_signature([(n, system.nl, system.nr, system.n_layers, 0, 0)], "fp32-product/" + precision, gpu)
+
+        def measure(_bps: int, order: str) -> float:
+            engine.set_fp32_product_path(n, 1 if order == "tcgen05" else 0)
+            system.transmission(omega, k_index, eta, precision=precision)  # warm-up
+            best = float("inf")
+            for _ in range(reps):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                system.transmission(omega, k_index, eta, precision=precision)
+                e1.record()
+                torch.cuda.synchronize()
+                best = min(best, e0.elapsed_time(e1))
+            return best
+
+        entry = self.select(key, measure, force)
+        path = 1 if entry["order"] == "tcgen05" else 0
+        engine.set_fp32_product_path(n, path)
+        return dict(entry, path=path)

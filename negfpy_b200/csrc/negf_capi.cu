@@ -331,6 +331,16 @@ int negf_cgemm_tf32x3(int n, int batch, const float* a, const float* b, float* c
   return 0;
 }
 
+int negf_set_fp32_product_path(int n, int path) {
+  if (n <= 0 || n > 256 || path < -1 || path > 1)
+    return fail(NEGF_EINVAL, "negf_set_fp32_product_path: order 1..256 and path -1, 0 or 1");
+  const int np = negf::mixed_order(n);
+  const int rc = negf::set_fp32_product_path(np, path);
+  if (rc == -2) return fail(NEGF_EUNSUPPORTED, "negf_set_fp32_product_path: tcgen05 tiles for orders up to 128 only");
+  if (rc < 0) return fail(NEGF_EINVAL, "negf_set_fp32_product_path: bad order");
+  return rc;
+}
+
 int negf_batch_max_grid(int max_order, int precision, int blocks_per_sm) {
   if (max_order <= 0 || max_order > 256 || (precision != 0 && precision != 1)) return 0;
   if (blocks_per_sm != 1 && blocks_per_sm != 2) return 0;

@@ -113,8 +113,11 @@ size_t rgf_mixed_ws_bytes(int np, int n, int grid);
 int rgf_mixed_launch(const RgfArgs& a, int np, int grid, void* ws, cudaStream_t st);
 
 namespace mixed {
-bool use_tc(int np);  // tcgen05 products at this padded order (<= 128, unless NEGF_TC=0)
+bool use_tc(int np);  // tcgen05 products at this padded order (see set_fp32_product_path)
 }
+// Product tiling of the FP32 sweeps at padded order np: -1 default, 0 mma.sync,
+// 1 tcgen05 (np <= 128).  Returns the effective path, -1 bad order, -2 unsupported.
+int set_fp32_product_path(int np, int path);
 // Refined device solve (FP32 factors, FP64 iterative refinement), orders 1..256.
 int rgf_refine_grid(int np);
 size_t rgf_refine_ws_bytes(int np, int n, int L, int grid);

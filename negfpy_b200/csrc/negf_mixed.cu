@@ -18,6 +18,7 @@
 //
 // A point whose FP32 sweep meets a singular or non-finite pivot reports the
 // status; the host re-solves those points with the FP64 kernel.
+#include <atomic>
 #include <cstdlib>
 
 #include "negf_common.cuh"
@@ -96,18 +97,29 @@ __global__ void __launch_bounds__(kThreads, 2) rgf_mixed_kernel(RgfArgs a, int N
 
 }  // namespace mixed
 
-// tcgen05 products for orders up to 128 unless NEGF_TC=0 (kept for A/B timing).
+// Product tiling of the FP32 sweeps per padded order (index np / 16):
+// -1 the default, 0 mma.sync 16 x 16 warp tiles, 1 tcgen05 128 x NP tiles
+// (orders up to 128).  Set by negf_set_fp32_product_path (the autotuner);
+// the default is mma.sync, or NEGF_TC=1 / 0 in the environment.
+std::atomic<int> g_fp32_path[17] = {-1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1};
 namespace mixed {
 bool use_tc(int np) {
+  if (np > tc::kMaxNP || np <= 0) return false;
+  const int v = g_fp32_path[np / 16].load();
+  if (v >= 0) return v == 1;
   static const int env = [] {
-    const char* v = getenv("NEGF_TC");
-    return (v && v[0] == '0') ? 0 : 1;
+    const char* e = getenv("NEGF_TC");
+    return (e && e[0] == '1') ? 1 : 0;
   }();
-  return env && np <= tc::kMaxNP;
+  return env == 1;
 }
-
 }  // namespace mixed
-
+int set_fp32_product_path(int np, int path) {
+  if (np <= 0 || np > 256 || np % 16 != 0) return -1;
+  if (path == 1 && np > tc::kMaxNP) return -2;
+  g_fp32_path[np / 16].store(path < 0 ? -1 : path);
+  return mixed::use_tc(np) ? 1 : 0;
+}
 int mixed_order(int n) {
   if (n <= 0 || n > 256) return 0;
   return (n + 15) / 16 * 16;

@@ -15,9 +15,10 @@
 // the instruction descriptor.  K runs in slabs of KS = 16: the block stages
 // a slab of both operands in shared memory (split and laid out in the
 // no-swizzle K-major core-matrix layout), one thread issues the slab's 24
-// MMAs and commits them to an mbarrier, every thread waits on it (at most
-// 2 s of wall time; then the product reports failure),
-// and the next slab is staged.  The result is read back with tcgen05.ld and
+// MMAs and commits them to an mbarrier while every thread loads the next
+// slab from global memory into registers, every thread waits on the barrier
+// (at most 2 s of wall time; then the product reports failure), and the next
+// slab is staged.  The result is read back with tcgen05.ld and
 // written to C.
 #pragma once
 #include "negf_common.cuh"
@@ -60,9 +61,46 @@ __device__ __forceinline__ void put_split(unsigned char* part0, uint32_t part_by
   *reinterpret_cast<unsigned*>(part0 + 3 * part_bytes + off) = il;
 }
 
+// Elements of one slab a thread stages: MT*KS of A and NP*KS of B over the
+// block's threads (at most kMaxNP).
+constexpr int kPerA = MT * KS / kThreads;
+constexpr int kPerB = kMaxNP * KS / kThreads;
+
+template <bool AC>
+__device__ __forceinline__ void load_a(float2 (&ra)[kPerA], const float2* __restrict__ A, int NP, int k0) {
+#pragma unroll
+  for (int i = 0; i < kPerA; ++i) {
+    const int e = threadIdx.x + i * kThreads;
+    int r, k;
+    if (AC) { k = e / MT; r = e - k * MT; } else { r = e / KS; k = e - r * KS; }
+    float2 v = make_float2(0.f, 0.f);
+    if (r < NP) {
+      v = AC ? A[(long long)(k0 + k) * NP + r] : A[(long long)r * NP + k0 + k];
+      if (AC) v.y = -v.y;
+    }
+    ra[i] = v;
+  }
+}
+template <bool BC>
+__device__ __forceinline__ void load_b(float2 (&rb)[kPerB], const float2* __restrict__ B, int NP, int k0) {
+#pragma unroll
+  for (int i = 0; i < kPerB; ++i) {
+    const int e = threadIdx.x + i * kThreads;
+    float2 v = make_float2(0.f, 0.f);
+    if (e < NP * KS) {
+      int n, k;
+      if (BC) { n = e / KS; k = e - n * KS; } else { k = e / NP; n = e - k * NP; }
+      v = BC ? B[(long long)n * NP + k0 + k] : B[(long long)(k0 + k) * NP + n];
+      if (BC) v.y = -v.y;
+    }
+    rb[i] = v;
+  }
+}
+
 // C = op(A) op(B).  Every thread of the block calls it; it ends with the
 // block synchronised.  Returns false if an mbarrier wait ran out (C is then
-// not valid; *ctx.err is set).
+// not valid; *ctx.err is set).  The global loads of slab s + 1 are issued
+// right after slab s's MMAs, so they overlap the MMAs and the wait.
 template <bool AC, bool BC>
 __device__ bool cprod(float2* __restrict__ C, const float2* __restrict__ A, const float2* __restrict__ B, int NP,
                       Ctx& ctx) {
@@ -75,24 +113,26 @@ __device__ bool cprod(float2* __restrict__ C, const float2* __restrict__ A, cons
   const uint32_t id_pos = umma::idesc_tf32(MT, NP, false), id_neg = umma::idesc_tf32(MT, NP, true);
   const uint32_t t_re = ctx.tmem, t_im = ctx.tmem + (uint32_t)NP;
   bool ok = true;
+  float2 ra[kPerA], rb[kPerB];
+  load_a<AC>(ra, A, NP, 0);
+  load_b<BC>(rb, B, NP, 0);
   for (int k0 = 0; k0 < NP; k0 += KS) {
     // stage op(A)[0:128, k0:k0+KS] and op(B)[k0:k0+KS, 0:NP] (as its transpose)
-    for (int e = tid; e < MT * KS; e += kThreads) {
+#pragma unroll
+    for (int i = 0; i < kPerA; ++i) {
+      const int e = tid + i * kThreads;
       int r, k;
       if (AC) { k = e / MT; r = e - k * MT; } else { r = e / KS; k = e - r * KS; }
-      float2 v = make_float2(0.f, 0.f);
-      if (r < NP) {
-        v = AC ? A[(long long)(k0 + k) * NP + r] : A[(long long)r * NP + k0 + k];
-        if (AC) v.y = -v.y;
-      }
-      put_split(sa, pa_bytes, core_off(r, k), v);
+      put_split(sa, pa_bytes, core_off(r, k), ra[i]);
     }
-    for (int e = tid; e < NP * KS; e += kThreads) {
-      int n, k;
-      if (BC) { n = e / KS; k = e - n * KS; } else { k = e / NP; n = e - k * NP; }
-      float2 v = BC ? B[(long long)n * NP + k0 + k] : B[(long long)(k0 + k) * NP + n];
-      if (BC) v.y = -v.y;
-      put_split(sb, pb_bytes, core_off(n, k), v);
+#pragma unroll
+    for (int i = 0; i < kPerB; ++i) {
+      const int e = tid + i * kThreads;
+      if (e < NP * KS) {
+        int n, k;
+        if (BC) { n = e / KS; k = e - n * KS; } else { k = e / NP; n = e - k * NP; }
+        put_split(sb, pb_bytes, core_off(n, k), rb[i]);
+      }
     }
     umma::fence_proxy_async();
     umma::fence_before_sync();
@@ -122,6 +162,10 @@ __device__ bool cprod(float2* __restrict__ C, const float2* __restrict__ A, cons
         umma::mma_tf32(t_im, ad[2], bd[0], id_pos, true);
       }
       umma::mma_commit(ctx.bar);
+    }
+    if (k0 + KS < NP) {  // next slab's operands, in flight during the MMAs
+      load_a<AC>(ra, A, NP, k0 + KS);
+      load_b<BC>(rb, B, NP, k0 + KS);
     }
     if (ok) {
       ok = umma::mbar_wait(ctx.bar, ctx.phase, kWaitLimitNs);

@@ -515,3 +515,15 @@ def cgemm_tf32x3(a: torch.Tensor, b: torch.Tensor, conj_a: bool = False, conj_b:
     _lib.check(lib.negf_cgemm_tf32x3(n, P, _lib.ptr(a), _lib.ptr(b), _lib.ptr(c), int(conj_a), int(conj_b),
                                      _lib.ptr(st), _lib.stream_handle(stream)), "negf_cgemm_tf32x3")
     return c, st
+
+
+def set_fp32_product_path(n: int, path: int) -> int:
+    """Product tiling of the FP32 device sweeps (mixed and refined) at block
+    order ``n``: 0 mma.sync warp tiles, 1 tcgen05 128 x n tiles (n <= 128),
+    -1 the default.  Process-wide (``negf_set_fp32_product_path``); returns
+    the path now in effect."""
+    lib = _lib.load()
+    rc = lib.negf_set_fp32_product_path(int(n), int(path))
+    if rc < 0:
+        _lib.check(rc, "negf_set_fp32_product_path")
+    return rc

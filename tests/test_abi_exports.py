@@ -33,3 +33,19 @@ def test_workspace_query_without_gpu_is_safe():
 
 def test_build_is_for_sm100a():
     assert "arch=compute_100a,code=sm_100a" in " ".join(_build.ARCH)
+
+
+def test_fp32_product_path_switch_without_gpu():
+    """The product-tiling switch is host state only: it validates the order
+    and the path, refuses tcgen05 tiles above order 128 and reports the path
+    in effect (padded orders share a setting)."""
+    lib = _lib.load()
+    assert lib.negf_set_fp32_product_path(48, 1) == 1
+    assert lib.negf_set_fp32_product_path(40, 0) == 0  # pads to 48
+    assert lib.negf_set_fp32_product_path(48, -1) in (0, 1)  # default: environment
+    assert lib.negf_set_fp32_product_path(160, 1) == -2  # NEGF_EUNSUPPORTED
+    assert "128" in lib.negf_last_error().decode()
+    assert lib.negf_set_fp32_product_path(160, 0) == 0
+    assert lib.negf_set_fp32_product_path(0, 0) == -1  # NEGF_EINVAL
+    assert lib.negf_set_fp32_product_path(48, 2) == -1
+    lib.negf_set_fp32_product_path(160, -1)
