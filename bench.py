@@ -32,6 +32,12 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 N_OMEGA, N_K, N_LAYERS = 2048, 64, 20
+_T0 = time.perf_counter()
+
+
+def _log(msg: str) -> None:
+    """Progress on stderr (the JSON line is the only stdout output)."""
+    print(f"[bench {time.perf_counter() - _T0:7.1f} s] {msg}", file=sys.stderr, flush=True)
 METRIC = "(omega,k)-points/s, FP64 transmission (SGF + RGF + trace), quasi-2D slab n=48"
 
 
@@ -51,6 +57,11 @@ def _args():
     ap.add_argument("--case", default="slab", choices=["slab", "bulk", "grad", "batch"],
                     help="slab: the benchmark; bulk / grad / batch: one small launch of each kernel family "
                          "(FP64 and mixed device solve at n=96, the adjoint, the uneven batch) for profiling")
+    ap.add_argument("--bulk-stride", type=int, default=8,
+                    help="refined-vs-FP64 comparison on every n-th omega of the 4096-omega bulk grid "
+                         "(1 = the full grid, about 8 minutes)")
+    ap.add_argument("--batch-stride", type=int, default=128,
+                    help="uneven batch on every n-th of its 1024 omegas per system (16 = about 9 minutes)")
     ap.add_argument("--kernels-only", action="store_true",
                     help="time the kernels only (no e2e, CPU baseline or peak probe); for profiling runs")
     return ap.parse_args()
@@ -272,6 +283,7 @@ def refined_vs_f64(torch, omega_stride=1, parity_points=512, cores=None, mixed_s
     res, ms = {}, {}
     for prec in ("f64", "refined"):
         res[prec], ms[prec] = timed(prec, allp)
+        _log(f"bulk {prec}: {P} points in {ms[prec] / 1e3:.1f} s")
     wm = np.arange(0, len(wi), mixed_stride)
     msel = torch.as_tensor((wm[:, None] * K + np.arange(K)[None, :]).ravel(), device="cuda")
     res["mixed"], ms["mixed"] = timed("mixed", msel)
@@ -316,6 +328,7 @@ def refined_vs_f64(torch, omega_stride=1, parity_points=512, cores=None, mixed_s
             t0 = time.perf_counter()
             t_or = O.transmission_points(wl, pairs, pool=pool)
             dt = time.perf_counter() - t0
+            _log(f"bulk oracle: {parity_points} points in {dt:.1f} s")
             rep = parity_report(t_or, t64.cpu().numpy()[pick],
                                 lambda idx: O.surface_residual_points(wl, [pairs[i] for i in idx], pool=pool))
         finally:
@@ -676,6 +689,7 @@ def main():
             events[2].record()
         return rl, T, st
 
+    _log(f"slab: {P} points per step, warm-up")
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
@@ -738,6 +752,7 @@ def main():
         roof["traffic"] = tr.get(dom)
         roof["traffic_source"] = "profiles/traffic.json (ncu, 4096-point case scaled to the launch)"
 
+    _log(f"timed steps done: {value:.4g} points/s")
     # End to end through the public API: per-k block construction on the host,
     # upload, GPU solve, result back to host.
     from negfpy_b200.models import material_kspace_device, material_kspace_lead
@@ -774,6 +789,7 @@ def main():
                "points_rel_diff_above_1e-8": int((e2e_rel > 1e-8).sum()),
                "kappa_300K_rel_diff_vs_device_run": abs(k_e2e - k_dev) / abs(k_dev)}
 
+    _log(f"e2e done: {e2e_val:.4g} points/s")
     cpu = None
     parity = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -785,7 +801,9 @@ def main():
         cpu = {"value": rate, "unit": "points/s", "cores": cores, "kind": "port",
                "sample": f"{nsamp} random points of the {W}x{K} grid ({dt:.1f} s wall); negfpy's algorithm "
                          "restated in oracle/ (numpy inv + SuperLU), spawn pool, 1 BLAS thread per process"}
+        _log(f"oracle CPU baseline: {nsamp} points in {dt:.1f} s")
         own = negfpy_rate(wl, shard, max(16 * cores, 128), cores)
+        _log("negfpy leg done")
         if own is not None:
             cpu["negfpy_own"] = own
         # The oracle's T at the sampled points against the timed run's FP64 T.
@@ -793,13 +811,18 @@ def main():
         gi = np.array([pos[a] * K + b for a, b in pairs])
         parity = parity_report(t_or, t_dev[gi], lambda idx: O.surface_residual_points(wl, [pairs[i] for i in idx]))
         parity["sample"] = f"the CPU baseline's {nsamp} random (omega,k) points; GPU T from the last timed step"
+    _log("parity report done")
     chain = chain_case(torch) if (rank == 0 and ws == 1 and not args.no_extras) else None
 
     extras = {}
     if ws == 1 and not args.no_extras:
-        extras["refined"] = refined_vs_f64(torch)
+        _log("chain done")
+        extras["refined"] = refined_vs_f64(torch, omega_stride=args.bulk_stride)
+        _log("refined done")
         extras["grad"] = grad_vs_forward(torch)
-        extras["uneven_batch"] = uneven_batch(torch)
+        _log("grad done")
+        extras["uneven_batch"] = uneven_batch(torch, omega_stride=args.batch_stride)
+        _log("uneven batch done")
 
     if rank == 0:
         out = {
