@@ -54,9 +54,12 @@ def _args():
                     help="omegas per rank (default: the full 2048; smaller values are profiling cases)")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the refined-precision and gradient measurements (run at N=1 only)")
-    ap.add_argument("--case", default="slab", choices=["slab", "bulk", "grad", "batch"],
-                    help="slab: the benchmark; bulk / grad / batch: one small launch of each kernel family "
-                         "(FP64 and mixed device solve at n=96, the adjoint, the uneven batch) for profiling")
+    ap.add_argument("--case", default="slab", choices=["slab", "bulk", "grad", "batch", "tc"],
+                    help="slab: the benchmark; bulk / grad / batch / tc: one small launch of each kernel family "
+                         "(FP64, mixed and refined device solve at n=96, the adjoints, the uneven batch, the "
+                         "tcgen05 products) for profiling")
+    ap.add_argument("--profile-omegas", type=int, default=16,
+                    help="omegas of the bulk and tc profiling cases (x 256 k-points)")
     ap.add_argument("--bulk-stride", type=int, default=8,
                     help="refined-vs-FP64 comparison on every n-th omega of the 4096-omega bulk grid "
                          "(1 = the full grid, about 8 minutes)")
@@ -544,21 +547,44 @@ def uneven_batch(torch, omega_stride=16, oracle_per_system=2):
             "launch": "one persistent kernel per solve, replayed from a CUDA graph; shape and order autotuned"}
 
 
-def profile_case(name, torch):
+def profile_case(name, torch, n_omega=16):
     """One small launch of each kernel of a family (for ncu), with CUDA-event times."""
     from negfpy_b200 import engine, spectrum, workloads as Wm
 
     ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
     out = {"case": name}
-    if name == "bulk":
+    if name in ("bulk", "tc"):
         wl = Wm.bulk_workload()
         s = engine.StackedSystem.from_arrays(wl.lead_l, wl.lead_l, wl.onsite, wl.coupling, wl.n_layers)
-        wi = np.arange(3, wl.omegas.size, 256)
+        wi = np.arange(3, wl.omegas.size, wl.omegas.size // n_omega)[:n_omega]
         K = len(wl.kpoints)
         om_w = torch.tensor(wl.omegas[wi], dtype=torch.float64, device="cuda")
         w_idx, k_idx = spectrum.grid_points(len(wi), K, om_w.device)
         om = om_w[w_idx].contiguous()
         eta = torch.full_like(om, wl.eta)
+    if name == "tc":
+        # the complex products alone (one per point's block order), then the
+        # FP32 sweeps with their products on tcgen05 tiles
+        n = s.n
+        gen = torch.Generator(device="cpu").manual_seed(3)
+        a = torch.randn((int(om.numel()), n, n), dtype=torch.complex64, generator=gen).cuda()
+        e = [ev() for _ in range(4)]
+        rl = engine.sgf_sr(*s.lead_l, om, eta, k_idx)
+        engine.set_fp32_product_path(n, 1)
+        e[0].record()
+        engine.cgemm_tf32x3(a, a, False, True)
+        e[1].record()
+        engine.rgf_transmission(s.onsite, s.coupling, s.n_layers, s.vl, s.vr, rl["g"], rl["g"], om, eta, k_idx,
+                                rl["status"], precision="mixed")
+        e[2].record()
+        engine.rgf_transmission_refine64(s.onsite, s.coupling, s.n_layers, s.vl, s.vr, rl["g"], rl["g"], om, eta,
+                                         k_idx, rl["status"])
+        e[3].record()
+        torch.cuda.synchronize()
+        engine.set_fp32_product_path(n, -1)
+        out.update(points=int(om.numel()), cgemm_ms=e[0].elapsed_time(e[1]), rgf_mixed_tc_ms=e[1].elapsed_time(e[2]),
+                   rgf_refined_tc_ms=e[2].elapsed_time(e[3]))
+    elif name == "bulk":
         e = [ev() for _ in range(5)]
         e[0].record()
         rl = engine.sgf_sr(*s.lead_l, om, eta, k_idx)
@@ -653,7 +679,7 @@ def main():
 
     if args.case != "slab":
         torch.cuda.set_device(0)
-        return profile_case(args.case, torch)
+        return profile_case(args.case, torch, args.profile_omegas)
     import torch.distributed as dist
 
     ws, rank, local = _dist()

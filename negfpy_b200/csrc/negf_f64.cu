@@ -295,10 +295,28 @@ struct GJShared {
   int* pivlog;    // pivlog[k]: logical row interchanged with row k at step k
   int* cmap;      // cmap[c] = t_k(...t_0(c)) over the steps done so far
   int* cmapinv;   // its inverse
-  unsigned* key;  // [8] pivot key of each panel column
+  unsigned* key;  // [8][NWB] each warp's pivot key of each panel column
 };
 template <int NP>
-__host__ __device__ constexpr int gj_shared_bytes() { return 5 * NP * 4 + 8 * 4; }
+__host__ __device__ constexpr int gj_shared_bytes() { return 5 * NP * 4 + 8 * Geo<NP>::NWB * 4; }
+// Pivot key of a panel column: the maximum of the warps' keys in `row`
+// (NWB entries, 16-byte aligned when NWB is a multiple of 4).
+template <int NP>
+__device__ __forceinline__ unsigned gj_key(const unsigned* row) {
+  constexpr int NWB = Geo<NP>::NWB;
+  unsigned k = 0u;
+  if constexpr (NWB % 4 == 0) {
+#pragma unroll
+    for (int w = 0; w < NWB; w += 4) {
+      const uint4 v = *reinterpret_cast<const uint4*>(row + w);
+      k = max(k, max(max(v.x, v.y), max(v.z, v.w)));
+    }
+  } else {
+#pragma unroll
+    for (int w = 0; w < NWB; ++w) k = max(k, row[w]);
+  }
+  return k;
+}
 template <int NP>
 __device__ __forceinline__ GJShared carve_gj(unsigned char* base) {
   GJShared g;
@@ -411,15 +429,15 @@ __device__ int gj_invert(double2* X, double2* Y, double2* Z, int n, const Lane& 
       sh.sig[r] = r;
       sh.siginv[r] = r;
     }
-    if (tid < 8) sh.key[tid] = 0u;
-    __syncthreads();
+    // Each warp posts its key in its own slot (no shared atomics); every
+    // thread takes the maximum over the slots after the barrier.
     key0 = __reduce_max_sync(0xffffffffu, key0);
-    if (lane == 0 && key0) atomicMax(&sh.key[0], key0);
+    if (lane == 0) sh.key[tid >> 5] = key0;
     __syncthreads();
     double2 lam = make_double2(1.0, 0.0);
     // ---- factor the panel, one barrier per column ----
     for (int j = 0; j < jmax; ++j) {
-      const unsigned key = sh.key[j];
+      const unsigned key = gj_key<NP>(sh.key + j * Geo<NP>::NWB);
       if ((key >> 20) >= 0x7ffu) return kNonFinite;
       if ((key >> 6) == 0u) return kSingular;
       const int pr = 63 - (int)(key & 63u);
@@ -467,7 +485,7 @@ __device__ int gj_invert(double2* X, double2* Y, double2* Z, int n, const Lane& 
       lam = cmul(lam, ps);
       if (j + 1 < jmax) {
         nk = __reduce_max_sync(0xffffffffu, nk);
-        if (lane == 0 && nk) atomicMax(&sh.key[j + 1], nk);
+        if (lane == 0) sh.key[(j + 1) * Geo<NP>::NWB + (tid >> 5)] = nk;
       }
       __syncthreads();
       double2* t = P;

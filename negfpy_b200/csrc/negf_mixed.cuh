@@ -127,9 +127,11 @@ struct GJS32 {
   int* sig;
   int* siginv;
   int* pivlog;
-  unsigned* key;
+  unsigned* key;  // [8][kWarps] each warp's pivot key of each panel column
 };
-__host__ __device__ inline size_t gjs32_bytes(int np) { return (size_t)2 * np * 8 * 8 + 3 * np * 4 + 8 * 4; }
+__host__ __device__ inline size_t gjs32_bytes(int np) {
+  return (size_t)2 * np * 8 * 8 + 3 * np * 4 + 8 * glob::kWarps * 4;
+}
 __device__ __forceinline__ GJS32 carve32(unsigned char* base, int np) {
   GJS32 s;
   s.panel = reinterpret_cast<float2*>(base);
@@ -178,10 +180,8 @@ static __device__ int gj_invert32(float2* X, float2* Y, int n, int NP, const GJS
       sh.sig[r] = r;
       sh.siginv[r] = r;
     }
-    if (tid < 8) sh.key[tid] = 0u;
-    __syncthreads();
     key0 = __reduce_max_sync(0xffffffffu, key0);
-    if (lane == 0 && key0) atomicMax(&sh.key[0], key0);
+    if (lane == 0) sh.key[warp] = key0;
     __syncthreads();
     float2 lam = make_float2(1.f, 0.f);
     // Bit i: row (tid >> 3) + 32 i (this thread's rows; its column is
@@ -189,7 +189,7 @@ static __device__ int gj_invert32(float2* X, float2* Y, int n, int NP, const GJS
     static_assert(kThreads == 256, "rows of a thread are 32 apart");
     unsigned used_rows = 0u;
     for (int j = 0; j < jmax; ++j) {
-      const unsigned key = sh.key[j];
+      const unsigned key = glob::key_max(sh.key + j * glob::kWarps);
       if ((key >> 23) >= 0xffu) return kNonFinite;
       if ((key >> 8) == 0u) return kSingular;
       const int pr = 255 - (int)(key & 255u);
@@ -224,7 +224,7 @@ static __device__ int gj_invert32(float2* X, float2* Y, int n, int NP, const GJS
       lam = fmulc(lam, ps);
       if (j + 1 < jmax) {
         nk = __reduce_max_sync(0xffffffffu, nk);
-        if (lane == 0 && nk) atomicMax(&sh.key[j + 1], nk);
+        if (lane == 0) sh.key[(j + 1) * glob::kWarps + warp] = nk;
       }
       __syncthreads();
       float2* t = P;

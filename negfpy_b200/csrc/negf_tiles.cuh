@@ -126,9 +126,24 @@ struct GJS {
   int* sig;
   int* siginv;
   int* pivlog;
-  unsigned* key;
+  unsigned* key;  // [8][kWarps] each warp's pivot key of each panel column
 };
-__host__ __device__ inline size_t gjs_bytes(int np) { return (size_t)2 * np * 8 * 16 + 3 * np * 4 + 8 * 4; }
+__host__ __device__ inline size_t gjs_bytes(int np) {
+  return (size_t)2 * np * 8 * 16 + 3 * np * 4 + 8 * kWarps * 4;
+}
+// Pivot key of a panel column: the maximum of the kWarps warp keys in `row`
+// (16-byte aligned).  Each warp posts its key in its own slot, so no shared
+// atomics are needed.
+__device__ __forceinline__ unsigned key_max(const unsigned* row) {
+  static_assert(kWarps % 4 == 0, "key slots are read 4 at a time");
+  unsigned k = 0u;
+#pragma unroll
+  for (int w = 0; w < kWarps; w += 4) {
+    const uint4 v = *reinterpret_cast<const uint4*>(row + w);
+    k = max(k, max(max(v.x, v.y), max(v.z, v.w)));
+  }
+  return k;
+}
 __device__ __forceinline__ GJS carve(unsigned char* base, int np) {
   GJS s;
   s.panel = reinterpret_cast<double2*>(base);
@@ -168,10 +183,8 @@ static __device__ int gj_invert_global(double2* X, double2* Y, int n, int NP, co
       sh.sig[r] = r;
       sh.siginv[r] = r;
     }
-    if (tid < 8) sh.key[tid] = 0u;
-    __syncthreads();
     key0 = __reduce_max_sync(0xffffffffu, key0);
-    if (lane == 0 && key0) atomicMax(&sh.key[0], key0);
+    if (lane == 0) sh.key[warp] = key0;
     __syncthreads();
     double2 lam = make_double2(1.0, 0.0);
     // Bit i: row (tid >> 3) + 32 i (this thread's rows; its column is
@@ -179,7 +192,7 @@ static __device__ int gj_invert_global(double2* X, double2* Y, int n, int NP, co
     static_assert(kThreads == 256, "rows of a thread are 32 apart");
     unsigned used_rows = 0u;
     for (int j = 0; j < jmax; ++j) {
-      const unsigned key = sh.key[j];
+      const unsigned key = key_max(sh.key + j * kWarps);
       if ((key >> 20) >= 0x7ffu) return kNonFinite;
       if ((key >> 8) == 0u) return kSingular;
       const int pr = 255 - (int)(key & 255u);
@@ -214,7 +227,7 @@ static __device__ int gj_invert_global(double2* X, double2* Y, int n, int NP, co
       lam = cmul(lam, ps);
       if (j + 1 < jmax) {
         nk = __reduce_max_sync(0xffffffffu, nk);
-        if (lane == 0 && nk) atomicMax(&sh.key[j + 1], nk);
+        if (lane == 0) sh.key[(j + 1) * kWarps + warp] = nk;
       }
       __syncthreads();
       double2* t = P;
