@@ -341,6 +341,84 @@ __device__ __forceinline__ unsigned pivot_key(double2 v, int r) {
   return (hm & ~63u) | (unsigned)(63 - r);
 }
 
+// Rank-8 update of one 16 x 16 tile (halves jm) by the factored panel
+// W = lambda P held in P (rows by physical row, sig: logical -> physical):
+//     next(r, Q) = [r not a pivot row] cur(sig r, Q) + P(sig r, :) W(sig(pivot rows), Q)
+//     next(r, panel) = P(sig r, :)
+// with P = W / lambda.  The half holding the panel's columns only stores
+// P(sig r, :) (its rank-8 sum would be discarded).
+template <int NP>
+__device__ __forceinline__ void rank8_tile(const double2* cur, double2* nxt, const double2* P, const int* sig,
+                                           double2 lam, int k0, int jmax, const Lane& T, int jm) {
+  const int ph = ((k0 >> 4) == (T.n0 >> 4)) ? ((k0 >> 3) & 1) : -1;  // the panel's half of this tile
+  const double2 il = crecip_smith(lam);
+  int srow[2];
+  bool inpanel[2];
+#pragma unroll
+  for (int ri = 0; ri < 2; ++ri) {
+    const int r = T.m0 + T.g + 8 * ri;
+    srow[ri] = sig[r];
+    inpanel[ri] = r >= k0 && r < k0 + jmax;
+  }
+  double ar[4], ai[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const double2 v = cmul(P[pidx(srow[q & 1], T.t + 4 * (q >> 1))], il);
+    ar[q] = v.x;
+    ai[q] = v.y;
+  }
+  const int kk0 = T.t, kk1 = T.t + 4;
+  const int pr0 = kk0 < jmax ? sig[k0 + kk0] : 0, pr1 = kk1 < jmax ? sig[k0 + kk1] : 0;
+#pragma unroll
+  for (int j2 = 0; j2 < 2; ++j2) {
+    if (!((jm >> j2) & 1)) continue;
+    if (j2 == ph) {
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int cc = own_c(T, j2, q);
+        nxt[sidx<NP>(own_r(T, q), cc)] = cmul(P[pidx(srow[q >> 1], cc - k0)], il);
+      }
+      continue;
+    }
+    double cr[4], ci[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const double2 v = cur[sidx<NP>(srow[q >> 1], own_c(T, j2, q))];
+      cr[q] = inpanel[q >> 1] ? 0.0 : v.x;
+      ci[q] = inpanel[q >> 1] ? 0.0 : v.y;
+    }
+    const int cc = T.n0 + 8 * j2 + T.g;
+    const double2 v0 = cur[sidx<NP>(pr0, cc)], v1 = cur[sidx<NP>(pr1, cc)];
+    double br[2], bi[2];
+    br[0] = kk0 < jmax ? v0.x : 0.0;
+    bi[0] = kk0 < jmax ? v0.y : 0.0;
+    br[1] = kk1 < jmax ? v1.x : 0.0;
+    bi[1] = kk1 < jmax ? v1.y : 0.0;
+    cmma(cr, ci, ar, ai, br, bi);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) nxt[sidx<NP>(own_r(T, q), own_c(T, j2, q))] = make_double2(cr[q], ci[q]);
+  }
+}
+
+// Rank-8 work split: at NP = 48 (9 tile warps in 12) the right half of tile
+// 8 moves from sub-partition 0 to warp 10 (sub-partition 2), which owns no
+// tile and does no Gauss-Jordan bookkeeping.
+template <int NP>
+struct R8Split {
+  static constexpr bool on = Geo<NP>::NW == 9 && Geo<NP>::NWB >= 11;
+  int jm;      // halves to compute: of the own tile, or the moved half (2)
+  bool extra;  // this warp takes the moved half
+  Lane Lx;     // the moved half's tile (use with j = 1)
+  __device__ __forceinline__ explicit R8Split(const Lane& L) {
+    const int w = threadIdx.x >> 5;
+    extra = on && w == Geo<NP>::NW + 1;
+    jm = extra ? 2 : ((on && w == Geo<NP>::NW - 1) ? 1 : 3);
+    Lx = L;
+    Lx.m0 = ((Geo<NP>::NW - 1) / Geo<NP>::T) * 16;
+    Lx.n0 = ((Geo<NP>::NW - 1) % Geo<NP>::T) * 16;
+  }
+};
+
 // Inverse of the leading n x n block of X (padding = identity, n <= NP <= 64)
 // by blocked Gauss-Jordan elimination with partial pivoting.  Y is the second
 // matrix buffer and Z (at least 2 NP x 8 complex) holds the panel; *out
@@ -377,6 +455,7 @@ __device__ int gj_invert(double2* X, double2* Y, double2* Z, int n, const Lane& 
   constexpr int PE = NP * 8;                  // panel elements
   constexpr int PPT = (PE + NTH - 1) / NTH;   // panel elements per thread
   const int tid = threadIdx.x, lane = tid & 31;
+  const R8Split<NP> r8(L);
   double2* cur = X;
   double2* nxt = Y;
   int rows[2], rbase[2], rsw[2];
@@ -492,59 +571,11 @@ __device__ int gj_invert(double2* X, double2* Y, double2* Z, int n, const Lane& 
       P = Pn;
       Pn = t;
     }
-    // ---- rank-8 update of the whole matrix (tile warps) ----
-    if (tw) {
-    const double2 il = crecip_smith(lam);
-    CAcc c;
-    int srow[2];
-    bool inpanel[2];
-#pragma unroll
-    for (int ri = 0; ri < 2; ++ri) {
-      srow[ri] = sh.sig[rows[ri]];
-      inpanel[ri] = rows[ri] >= k0 && rows[ri] < k0 + jmax;
-    }
-#pragma unroll
-    for (int j2 = 0; j2 < 2; ++j2)
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int ri = q >> 1, cc = own_c(L, j2, q);
-        const double2 v = cur[sidx<NP>(srow[ri], cc)];
-        c.re[j2][q] = inpanel[ri] ? 0.0 : v.x;
-        c.im[j2][q] = inpanel[ri] ? 0.0 : v.y;
-      }
-    {
-      double ar[4], ai[4];
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int kk = L.t + 4 * (q >> 1);
-        const double2 v = cmul(P[pidx(srow[q & 1], kk)], il);
-        ar[q] = v.x;
-        ai[q] = v.y;
-      }
-      const int kk0 = L.t, kk1 = L.t + 4;
-      const int pr0 = kk0 < jmax ? sh.sig[k0 + kk0] : 0, pr1 = kk1 < jmax ? sh.sig[k0 + kk1] : 0;
-#pragma unroll
-      for (int j2 = 0; j2 < 2; ++j2) {
-        const int cc = L.n0 + 8 * j2 + L.g;
-        const double2 v0 = cur[sidx<NP>(pr0, cc)], v1 = cur[sidx<NP>(pr1, cc)];
-        double br[2], bi[2];
-        br[0] = kk0 < jmax ? v0.x : 0.0;
-        bi[0] = kk0 < jmax ? v0.y : 0.0;
-        br[1] = kk1 < jmax ? v1.x : 0.0;
-        bi[1] = kk1 < jmax ? v1.y : 0.0;
-        cmma(c.re[j2], c.im[j2], ar, ai, br, bi);
-      }
-    }
-#pragma unroll
-    for (int j2 = 0; j2 < 2; ++j2)
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int r = own_r(L, q), cc = own_c(L, j2, q);
-        double2 v = c.get(j2, q);
-        if (cc >= k0 && cc < k0 + 8) v = cmul(P[pidx(srow[q >> 1], cc - k0)], il);
-        nxt[sidx<NP>(r, cc)] = v;
-      }
-    }
+    // ---- rank-8 update of the whole matrix ----
+    // The tile warps take their tiles; at NP = 48 the right half of the last
+    // tile goes to a warp without a tile on another sub-partition (kR8Helper),
+    // so that sub-partition 0 carries 5 halves instead of 6.
+    if (tw || r8.extra) rank8_tile<NP>(cur, nxt, P, sh.sig, lam, k0, jmax, r8.extra ? r8.Lx : L, r8.jm);
     // The panel's interchanges t_k = (k pivlog_k) applied to the column map,
     // by the bookkeeping thread (at n = 48 a warp without rank-8 work):
     // cmap <- t_k o cmap swaps the two entries holding the values k and b.
