@@ -516,33 +516,32 @@ __device__ int gj_invert(double2* X, double2* Y, double2* Z, int n, const Lane& 
     double2 lam = make_double2(1.0, 0.0);
     // ---- factor the panel, one barrier per column ----
     for (int j = 0; j < jmax; ++j) {
+      // The own elements do not depend on the pivot: load them with the key.
+      double2 mv[PPT], fv[PPT], av[PPT];
+#pragma unroll
+      for (int q = 0; q < PPT; ++q) {
+        fv[q] = P[pidx(pr_[q], j)];
+        av[q] = P[pidx(pr_[q], pc_[q])];
+      }
       const unsigned key = gj_key<NP>(sh.key + j * Geo<NP>::NWB);
       if ((key >> 20) >= 0x7ffu) return kNonFinite;
       if ((key >> 6) == 0u) return kSingular;
       const int pr = 63 - (int)(key & 63u);
       const int ex = (int)(key >> 20);
       const double sc = (ex != 0 && ex < 2046) ? __hiloint2double((2046 - ex) << 20, 0) : 1.0;
-      // Row interchange bookkeeping by the last warp: at n = 48 a warp with
-      // no product tile, which also keeps the column map during the rank-8
-      // update.
-      if (tid == NTH - 32) {
-        const int k = k0 + j;
-        const int bl = sh.siginv[pr];
-        const int pa = sh.sig[k];
-        sh.sig[k] = pr;
-        sh.sig[bl] = pa;
-        sh.siginv[pr] = k;
-        sh.siginv[pa] = bl;
-        sh.pivlog[k] = bl;
+      // Row interchange bookkeeping by the last warp (at n = 48 a warp with
+      // no product tile): its two loads go out with the pivot row's, its
+      // stores after the element update.
+      const bool bk = (tid == NTH - 32);
+      const int k = k0 + j;
+      int bl = 0, pa = 0;
+      if (bk) {
+        bl = sh.siginv[pr];
+        pa = sh.sig[k];
       }
       const double2 piv = P[pidx(pr, j)];
-      double2 mv[PPT], fv[PPT], av[PPT];
 #pragma unroll
-      for (int q = 0; q < PPT; ++q) {
-        mv[q] = P[pidx(pr, pc_[q])];
-        fv[q] = P[pidx(pr_[q], j)];
-        av[q] = P[pidx(pr_[q], pc_[q])];
-      }
+      for (int q = 0; q < PPT; ++q) mv[q] = P[pidx(pr, pc_[q])];
       const double2 ps = make_double2(piv.x * sc, piv.y * sc);
       unsigned nk = 0u;
 #pragma unroll
@@ -565,6 +564,13 @@ __device__ int gj_invert(double2* X, double2* Y, double2* Z, int n, const Lane& 
       if (j + 1 < jmax) {
         nk = __reduce_max_sync(0xffffffffu, nk);
         if (lane == 0) sh.key[(j + 1) * Geo<NP>::NWB + (tid >> 5)] = nk;
+      }
+      if (bk) {
+        sh.sig[k] = pr;
+        sh.sig[bl] = pa;
+        sh.siginv[pr] = k;
+        sh.siginv[pa] = bl;
+        sh.pivlog[k] = bl;
       }
       __syncthreads();
       double2* t = P;
