@@ -299,24 +299,6 @@ struct GJShared {
 };
 template <int NP>
 __host__ __device__ constexpr int gj_shared_bytes() { return 5 * NP * 4 + 8 * Geo<NP>::NWB * 4; }
-// Pivot key of a panel column: the maximum of the warps' keys in `row`
-// (NWB entries, 16-byte aligned when NWB is a multiple of 4).
-template <int NP>
-__device__ __forceinline__ unsigned gj_key(const unsigned* row) {
-  constexpr int NWB = Geo<NP>::NWB;
-  unsigned k = 0u;
-  if constexpr (NWB % 4 == 0) {
-#pragma unroll
-    for (int w = 0; w < NWB; w += 4) {
-      const uint4 v = *reinterpret_cast<const uint4*>(row + w);
-      k = max(k, max(max(v.x, v.y), max(v.z, v.w)));
-    }
-  } else {
-#pragma unroll
-    for (int w = 0; w < NWB; ++w) k = max(k, row[w]);
-  }
-  return k;
-}
 template <int NP>
 __device__ __forceinline__ GJShared carve_gj(unsigned char* base) {
   GJShared g;
@@ -492,15 +474,21 @@ __device__ int gj_invert(double2* X, double2* Y, double2* Z, int n, const Lane& 
     double2* P = Z;
     double2* Pn = Z + PE;
     bool used[PPT];
+    // Each thread also keeps its own panel elements in registers (av), so a
+    // column step reads from shared memory only what other threads wrote:
+    // its row's entry of the pivot column and the pivot row.
+    double2 av[PPT];
     // ---- load the panel, reset the bookkeeping, keys of panel column 0 ----
     unsigned key0 = 0u;
 #pragma unroll
     for (int q = 0; q < PPT; ++q) {
       const int r = pr_[q], c = pc_[q];
       used[q] = false;
+      av[q] = make_double2(0.0, 0.0);
       if (pin[q]) {
         const double2 v = cur[sidx<NP>(r, k0 + c)];
         P[pidx(r, c)] = v;
+        av[q] = v;
         if (c == 0 && r >= k0 && r < n) key0 = max(key0, pivot_key(v, r));
       }
     }
@@ -508,22 +496,22 @@ __device__ int gj_invert(double2* X, double2* Y, double2* Z, int n, const Lane& 
       sh.sig[r] = r;
       sh.siginv[r] = r;
     }
-    // Each warp posts its key in its own slot (no shared atomics); every
-    // thread takes the maximum over the slots after the barrier.
+    // Each warp posts its key in its own slot (no shared atomics); after the
+    // barrier lane i of every warp reads slot i and the warp takes the max.
     key0 = __reduce_max_sync(0xffffffffu, key0);
     if (lane == 0) sh.key[tid >> 5] = key0;
     __syncthreads();
     double2 lam = make_double2(1.0, 0.0);
     // ---- factor the panel, one barrier per column ----
     for (int j = 0; j < jmax; ++j) {
-      // The own elements do not depend on the pivot: load them with the key.
-      double2 mv[PPT], fv[PPT], av[PPT];
+      // The own rows' pivot-column entries do not depend on the pivot: load
+      // them with the key.  The key slots are read one lane per slot and
+      // reduced in the warp (one shared-memory wavefront per warp).
+      double2 mv[PPT], fv[PPT];
 #pragma unroll
-      for (int q = 0; q < PPT; ++q) {
-        fv[q] = P[pidx(pr_[q], j)];
-        av[q] = P[pidx(pr_[q], pc_[q])];
-      }
-      const unsigned key = gj_key<NP>(sh.key + j * Geo<NP>::NWB);
+      for (int q = 0; q < PPT; ++q) fv[q] = P[pidx(pr_[q], j)];
+      const unsigned key =
+          __reduce_max_sync(0xffffffffu, lane < Geo<NP>::NWB ? sh.key[j * Geo<NP>::NWB + lane] : 0u);
       if ((key >> 20) >= 0x7ffu) return kNonFinite;
       if ((key >> 6) == 0u) return kSingular;
       const int pr = 63 - (int)(key & 63u);
@@ -558,6 +546,7 @@ __device__ int gj_invert(double2* X, double2* Y, double2* Z, int n, const Lane& 
         double2 v = cneg(cmul(b, m));
         if (!isp && c != j) cfma(v, ps, av[q]);
         Pn[pidx(r, c)] = v;
+        av[q] = v;
         if (c == j + 1 && !used[q] && r >= k0 && r < n) nk = max(nk, pivot_key(v, r));
       }
       lam = cmul(lam, ps);
