@@ -494,7 +494,30 @@ def uneven_batch(torch, omega_stride=16, oracle_per_system=2):
         out[prec] = {"points_per_s": P / ms * 1e3, "ms": ms, "blocks_per_sm": c["blocks_per_sm"],
                      "order": c["order"], "failed": int(bad.sum()), "fallback": nfb,
                      "tuning_ms": {k: round(v, 1) for k, v in c["timings"].items()}}
+        b.release(g)
         del g
+        # Split schedule: one launch per padded-order class, each tuned on its own.
+        plan = tuner.tune_split(b, prec, tune_oms, reps=1, force=True)
+        parts = b.split_parts(it, plan)
+        gs, (Ts, sts, _) = b.graph_split(parts, prec)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        gs.replay()
+        e1.record()
+        torch.cuda.synchronize()
+        ms_s = e0.elapsed_time(e1)
+        out[prec]["split"] = {
+            "points_per_s": P / ms_s * 1e3, "ms": ms_s,
+            "classes": {str(cl): {"blocks_per_sm": e["blocks_per_sm"], "order": e["order"],
+                                  "tuning_ms": {k: round(v, 1) for k, v in e["timings"].items()}}
+                        for cl, e in plan.items()},
+            "failed": int((sts != 0).sum()),
+            "T_bitwise_equal_to_single_launch": bool(torch.equal(Ts, Tc)) if nfb == 0 else None}
+        out[prec]["schedule"] = "split" if ms_s < ms else "single"
+        out[prec]["best_points_per_s"] = P / min(ms, ms_s) * 1e3
+        b.release(gs)
+        del gs
     offs = np.cumsum([0] + [o.size * len(w.kpoints) for o, w in zip(oms, ws)])
     errs = []
     for i, w in enumerate(ws):
@@ -544,7 +567,8 @@ def uneven_batch(torch, omega_stride=16, oracle_per_system=2):
             "kappa_rel_err_max": float(errs.max()), "kappa_rel_err_median": float(np.median(errs)),
             "kappa_err_reference": "the FP64 batch on the same omegas (kappa needs the whole omega grid)",
             "oracle_sample": oracle,
-            "launch": "one persistent kernel per solve, replayed from a CUDA graph; shape and order autotuned"}
+            "launch": "one persistent kernel per solve (or, in `split`, one per padded-order class), replayed "
+                      "from a CUDA graph; launch shape and item order autotuned, per class for the split schedule"}
 
 
 def profile_case(name, torch, n_omega=16):

@@ -11,6 +11,10 @@ CUDA events, keeps the fastest, and caches the choice in a JSON file keyed by
 the GPU, the precision and the shape of the batch (block orders, layer counts
 and k counts of its systems).
 
+``BatchTuner.tune_split`` makes the same choice per padded-order class for
+the split schedule (one launch per class), so the launch shape and item
+order can differ between block orders.
+
 The FP32 device sweeps (mixed and refined precision) have two product
 tilings for block orders up to 128: 16 x 16 warp tiles on mma.sync, or
 128 x n tiles on the tcgen05 tensor cores with TMEM accumulators.
@@ -115,6 +119,39 @@ class BatchTuner:
             return best
 
         return self.select(key, measure, force)
+
+    def tune_split(self, batch, precision: str, sample_omegas, reps: int = 2, force: bool = False) -> dict:
+        """The split schedule's plan: for every order class of ``batch`` the
+        (blocks_per_sm, order) that runs the class's items of
+        ``sample_omegas`` fastest on their own (launched with the class's
+        largest order), each cached under the shapes of the class's systems.
+        Returns {class: entry}."""
+        import torch
+
+        gpu = torch.cuda.get_device_name() + f"/{torch.cuda.get_device_properties(0).multi_processor_count}SM"
+        shapes = batch_shapes(batch)
+        plan = {}
+        for c, mo, sub in batch.class_items(batch.items(sample_omegas, "system")):
+            members = sorted(set(int(i) for i in sub.system.cpu().numpy()))
+            key = batch_signature([shapes[i] for i in members], f"{precision}/class", gpu)
+
+            def measure(bps: int, order: str, sub=sub, mo=mo) -> float:
+                if batch.max_grid(precision, bps, mo) <= 0:
+                    raise RuntimeError("launch shape not available")
+                it = sub.reordered(order)
+                batch.launch(it, precision, blocks_per_sm=bps, max_order=mo)  # warm-up
+                best = float("inf")
+                for _ in range(reps):
+                    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    e0.record()
+                    batch.launch(it, precision, blocks_per_sm=bps, max_order=mo)
+                    e1.record()
+                    torch.cuda.synchronize()
+                    best = min(best, e0.elapsed_time(e1))
+                return best
+
+            plan[c] = self.select(key, measure, force)
+        return plan
 
 
 class ProductPathTuner(BatchTuner):

@@ -16,7 +16,11 @@ per (omega, k)); an item is (system, k index, omega).  The host
   ``precision="refined"`` is the FP64-accurate reduced-precision solve.)
 
 Launch shapes (blocks per SM) and the item order come from
-``negfpy_b200.autotune``.
+``negfpy_b200.autotune``.  Two schedules: one launch over every item, or a
+split schedule of one launch per padded-order class (the items whose
+largest block order rounds up to the same multiple of 16), each class with
+its own launch shape and item order; the tuner chooses per class and
+between the schedules.
 """
 
 from __future__ import annotations
@@ -77,6 +81,12 @@ def item_order(system: np.ndarray, cost: np.ndarray, order: str) -> np.ndarray:
     raise ValueError(f"unknown item order {order!r}; expected 'lpt', 'system' or 'interleave'")
 
 
+def order_class(n: int, nl: int, nr: int) -> int:
+    """Padded block order of a system (its largest order rounded up to 16):
+    the class of its items in a split schedule."""
+    return (max(n, nl, nr) + 15) // 16 * 16
+
+
 @dataclass
 class Items:
     system: torch.Tensor  # int32 [P], launch order
@@ -84,6 +94,15 @@ class Items:
     omega: torch.Tensor   # float64 [P]
     perm: torch.Tensor    # int64 [P]: launch position -> caller's item index
     cost: np.ndarray      # estimated cost per item, launch order
+
+    def take(self, idx: np.ndarray) -> "Items":
+        """The items at launch positions ``idx``, in that order."""
+        sel = torch.as_tensor(idx, device=self.system.device)
+        return Items(self.system[sel].contiguous(), self.k[sel].contiguous(), self.omega[sel].contiguous(),
+                     self.perm[sel].contiguous(), self.cost[idx])
+
+    def reordered(self, order: str) -> "Items":
+        return self.take(item_order(self.system.cpu().numpy(), self.cost, order))
 
 
 class UnevenBatch:
@@ -114,6 +133,8 @@ class UnevenBatch:
         raw = torch.frombuffer(bytearray(C.string_at(C.addressof(arr), C.sizeof(arr))), dtype=torch.uint8)
         self.table = raw.to(dev)
         self.max_order = max(max(s.n, s.nl, s.nr) for s, _, _ in self.systems)
+        self.sys_class = np.array([order_class(s.n, s.nl, s.nr) for s, _, _ in self.systems], dtype=np.int64)
+        self.sys_order = np.array([max(s.n, s.nl, s.nr) for s, _, _ in self.systems], dtype=np.int64)
         self._graphs: dict = {}
 
     @staticmethod
@@ -161,28 +182,56 @@ class UnevenBatch:
         return Items(torch.as_tensor(sys_i[perm], device=dev), torch.as_tensor(k_i[perm], device=dev),
                      torch.as_tensor(om[perm], device=dev), torch.as_tensor(perm, device=dev), cost[perm])
 
+    def class_items(self, it: Items, orders=None) -> list:
+        """The items of each order class, as (class, max order, Items), classes
+        ascending.  Within a class the items keep their order in ``it``, or are
+        put in ``orders[class]`` ("lpt", "system" or "interleave")."""
+        sys_np = it.system.cpu().numpy()
+        cls = self.sys_class[sys_np]
+        out = []
+        for c in np.unique(cls):
+            idx = np.nonzero(cls == c)[0]
+            if orders is not None:
+                idx = idx[item_order(sys_np[idx], it.cost[idx], orders[int(c)])]
+            mo = int(self.sys_order[np.unique(sys_np[idx])].max())
+            out.append((int(c), mo, it.take(idx)))
+        return out
+
     # ----------------------------------------------------------------- launch
     def _buffers(self, P: int):
         dev = self.device
         return (torch.empty(P, dtype=torch.float64, device=dev), torch.empty(P, dtype=torch.int32, device=dev),
                 torch.empty(P, dtype=torch.int32, device=dev))
 
-    def max_grid(self, precision: str = "f64", blocks_per_sm: int = 1) -> int:
-        return int(_lib.load().negf_batch_max_grid(self.max_order, PRECISIONS[precision], int(blocks_per_sm)))
+    def max_grid(self, precision: str = "f64", blocks_per_sm: int = 1, max_order: int = 0) -> int:
+        mo = int(max_order) or self.max_order
+        return int(_lib.load().negf_batch_max_grid(mo, PRECISIONS[precision], int(blocks_per_sm)))
+
+    def workspace_bytes(self, precision: str = "f64", blocks_per_sm: int = 1, grid: int = 0, max_order: int = 0):
+        lib = _lib.load()
+        mo = int(max_order) or self.max_order
+        need = int(lib.negf_batch_workspace_bytes(mo, PRECISIONS[precision], int(blocks_per_sm), int(grid)))
+        if need == 0:
+            raise RuntimeError("negf_batch_workspace_bytes failed: " + lib.negf_last_error().decode())
+        return need
 
     def launch(self, it: Items, precision: str = "f64", grid: int = 0, tol: float = 1e-12, maxiter: int = 200,
-               out=None, stream=None, blocks_per_sm: int = 1):
+               out=None, stream=None, blocks_per_sm: int = 1, max_order: int = 0, ws=None):
         """One persistent launch over the items (launch order).  Returns
-        (T, status, iters) in launch order."""
+        (T, status, iters) in launch order.  ``max_order``: the largest block
+        order among the items' systems (default: the batch's); ``ws``: a
+        workspace of at least ``workspace_bytes`` (default: the cached one)."""
         lib = _lib.load()
         P = int(it.system.numel())
         T, st, iters = out if out is not None else self._buffers(P)
         prec = PRECISIONS[precision]
-        need = int(lib.negf_batch_workspace_bytes(self.max_order, prec, int(blocks_per_sm), int(grid)))
-        if need == 0:
-            raise RuntimeError("negf_batch_workspace_bytes failed: " + lib.negf_last_error().decode())
-        ws = engine._workspace(need, self.device, f"batch_{precision}")
-        rc = lib.negf_batch_transmission(self.table.data_ptr(), self.n_systems, self.max_order, it.system.data_ptr(),
+        mo = int(max_order) or self.max_order
+        need = self.workspace_bytes(precision, blocks_per_sm, grid, mo)
+        if ws is None:
+            ws = engine._workspace(need, self.device, f"batch_{precision}")
+        elif ws.numel() < need:
+            raise ValueError(f"batch workspace of {ws.numel()} bytes; {need} needed")
+        rc = lib.negf_batch_transmission(self.table.data_ptr(), self.n_systems, mo, it.system.data_ptr(),
                                          it.k.data_ptr(), it.omega.data_ptr(), P, float(tol), int(maxiter), prec,
                                          int(blocks_per_sm), int(grid), T.data_ptr(), st.data_ptr(), iters.data_ptr(), ws.data_ptr(),
                                          ws.numel(), _lib.stream_handle(stream))
@@ -195,17 +244,71 @@ class UnevenBatch:
         its output buffers; ``g.replay()`` re-solves the items."""
         P = int(it.system.numel())
         out = self._buffers(P)
-        # outside the capture: sizes the workspace and sets the kernel attributes
-        self.launch(it, precision, grid, tol, maxiter, out, blocks_per_sm=blocks_per_sm)
+        # the graph's own workspace, kept with the batch while the graph lives
+        ws = torch.empty(self.workspace_bytes(precision, blocks_per_sm, grid), dtype=torch.uint8, device=self.device)
+        # outside the capture: sets the kernel attributes
+        self.launch(it, precision, grid, tol, maxiter, out, blocks_per_sm=blocks_per_sm, ws=ws)
         torch.cuda.synchronize()
         g = torch.cuda.CUDAGraph()
         s = torch.cuda.Stream()
         s.wait_stream(torch.cuda.current_stream())
         with torch.cuda.stream(s):
             with torch.cuda.graph(g, stream=s):
-                self.launch(it, precision, grid, tol, maxiter, out, blocks_per_sm=blocks_per_sm)
+                self.launch(it, precision, grid, tol, maxiter, out, blocks_per_sm=blocks_per_sm, ws=ws)
         torch.cuda.current_stream().wait_stream(s)
+        self._graphs[id(g)] = ws
         return g, out
+
+    # ------------------------------------------------------- split schedule
+    def split_parts(self, it: Items, plan: dict | None = None) -> list:
+        """The launches of the split schedule for ``it``: (class, max order,
+        Items in the class's order, blocks per SM) per order class, from
+        ``plan`` ({class: {"blocks_per_sm": b, "order": o}}; default one block
+        per SM, largest cost first)."""
+        plan = plan or {}
+        orders = {int(c): plan.get(int(c), {}).get("order", "lpt") for c in np.unique(self.sys_class)}
+        return [(c, mo, sub, int(plan.get(c, {}).get("blocks_per_sm", 1)))
+                for c, mo, sub in self.class_items(it, orders)]
+
+    def split_workspace_bytes(self, parts, precision: str = "f64") -> int:
+        return max(self.workspace_bytes(precision, bps, 0, mo) for _, mo, _, bps in parts)
+
+    def launch_split(self, parts, precision: str = "f64", tol: float = 1e-12, maxiter: int = 200, out=None,
+                     ws=None):
+        """The split schedule's launches, one after the other on the current
+        stream.  Returns (T, status, iters) in the CALLER's item order (the
+        class launches scatter their results through their ``perm``)."""
+        P = sum(int(sub.system.numel()) for _, _, sub, _ in parts)
+        T, st, iters = out if out is not None else self._buffers(P)
+        for _, mo, sub, bps in parts:
+            t, s_, i_ = self.launch(sub, precision, 0, tol, maxiter, blocks_per_sm=bps, max_order=mo, ws=ws)
+            T[sub.perm] = t
+            st[sub.perm] = s_
+            iters[sub.perm] = i_
+        return T, st, iters
+
+    def graph_split(self, parts, precision: str = "f64", tol: float = 1e-12, maxiter: int = 200):
+        """A CUDA graph of the split schedule (its own workspace, kept with the
+        batch while the graph lives); ``g.replay()`` re-solves the items.
+        Returns the graph and its (T, status, iters) in the caller's order."""
+        P = sum(int(sub.system.numel()) for _, _, sub, _ in parts)
+        out = self._buffers(P)
+        ws = torch.empty(self.split_workspace_bytes(parts, precision), dtype=torch.uint8, device=self.device)
+        self.launch_split(parts, precision, tol, maxiter, out, ws)  # kernel attributes, outside the capture
+        torch.cuda.synchronize()
+        g = torch.cuda.CUDAGraph()
+        s = torch.cuda.Stream()
+        s.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(s):
+            with torch.cuda.graph(g, stream=s):
+                self.launch_split(parts, precision, tol, maxiter, out, ws)
+        torch.cuda.current_stream().wait_stream(s)
+        self._graphs[id(g)] = ws
+        return g, out
+
+    def release(self, g) -> None:
+        """Drop the workspace kept for graph ``g`` (do not replay it afterwards)."""
+        self._graphs.pop(id(g), None)
 
     def solve(self, it: Items, precision: str = "f64", grid: int = 0, tol: float = 1e-12,
               maxiter: int = 200, blocks_per_sm: int = 1) -> dict:

@@ -69,3 +69,29 @@ def test_uneven_workload_shapes():
         assert w.omegas.size == 16 and w.omegas.max() <= 1.05 * w.omega_max + 1e-12
         d = w.lead_l["d00"][0]
         assert np.abs(d - d.conj().T).max() < 1e-12
+
+
+def test_order_classes_and_split_parts():
+    """Items grouped by padded block order, each class in its own item order,
+    with the launch shape of its plan entry (a batch object without device
+    state: class_items and split_parts are host logic)."""
+    import torch
+
+    from negfpy_b200.batch import Items, UnevenBatch, order_class
+
+    assert [order_class(24, 24, 24), order_class(48, 48, 48), order_class(72, 48, 72), order_class(120, 96, 96)] == \
+        [32, 48, 80, 128]
+    b = UnevenBatch.__new__(UnevenBatch)
+    b.device = torch.device("cpu")
+    b.sys_class = np.array([32, 48, 32, 192])
+    b.sys_order = np.array([24, 48, 30, 192])
+    system = np.array([0, 1, 2, 3, 0, 3, 2])
+    cost = np.array([1.0, 2.0, 3.0, 9.0, 1.5, 8.0, 0.5])
+    it = Items(torch.as_tensor(system, dtype=torch.int32), torch.zeros(7, dtype=torch.int32),
+               torch.arange(7, dtype=torch.float64), torch.arange(7) + 100, cost)
+    parts = b.split_parts(it, {192: {"blocks_per_sm": 2, "order": "system"}})
+    assert [(c, mo, bps) for c, mo, _, bps in parts] == [(32, 30, 1), (48, 48, 1), (192, 192, 2)]
+    sub32 = parts[0][2]
+    assert list(sub32.perm.numpy()) == [102, 104, 100, 106]  # lpt inside the class: costs 3, 1.5, 1, 0.5
+    assert list(parts[2][2].perm.numpy()) == [103, 105]        # "system": the given order
+    assert sum(int(p[2].system.numel()) for p in parts) == 7

@@ -140,3 +140,32 @@ def test_tuner_on_gpu(small, tmp_path):
     c = tuner.tune(b, "mixed", [w.omegas[:3] for w in ws], reps=1)
     assert c["blocks_per_sm"] in (1, 2) and c["order"] in ("lpt", "interleave", "system") and not c["cached"]
     assert tuner.tune(b, "mixed", [w.omegas[:3] for w in ws])["cached"]
+
+
+def test_split_schedule_matches_single_launch(small, tmp_path):
+    """The split schedule (one launch per padded-order class, each with its
+    own tuned launch shape and order) gives every item bitwise the same T as
+    the single launch, directly and replayed from its CUDA graph; the tuner
+    returns one cached entry per class."""
+    from negfpy_b200.autotune import BatchTuner
+
+    ws, b = small
+    it = b.items([w.omegas for w in ws], "lpt")
+    T1, s1, _ = b.launch(it, "f64")
+    single = torch.empty_like(T1)
+    single[it.perm] = T1
+    tuner = BatchTuner(tmp_path / "tune.json")
+    plan = tuner.tune_split(b, "f64", [w.omegas[:2] for w in ws], reps=1)
+    assert sorted(plan) == sorted(set(int(c) for c in b.sys_class))
+    assert all(e["blocks_per_sm"] in (1, 2) and not e["cached"] for e in plan.values())
+    assert all(e["cached"] for e in tuner.tune_split(b, "f64", [w.omegas[:2] for w in ws]).values())
+    parts = b.split_parts(it, plan)
+    assert sum(int(sub.system.numel()) for _, _, sub, _ in parts) == int(it.system.numel())
+    T2, s2, _ = b.launch_split(parts, "f64")
+    assert torch.equal(T2, single) and int((s2 != 0).sum()) == 0
+    g, (T3, _, _) = b.graph_split(parts, "f64")
+    T3.fill_(-1.0)
+    g.replay()
+    torch.cuda.synchronize()
+    assert torch.equal(T3, single)
+    b.release(g)
