@@ -497,27 +497,30 @@ def uneven_batch(torch, omega_stride=16, oracle_per_system=2):
         b.release(g)
         del g
         # Split schedule: one launch per padded-order class, each tuned on its own.
-        plan = tuner.tune_split(b, prec, tune_oms, reps=1, force=True)
-        parts = b.split_parts(it, plan)
-        gs, (Ts, sts, _) = b.graph_split(parts, prec)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        torch.cuda.synchronize()
-        e0.record()
-        gs.replay()
-        e1.record()
-        torch.cuda.synchronize()
-        ms_s = e0.elapsed_time(e1)
-        out[prec]["split"] = {
-            "points_per_s": P / ms_s * 1e3, "ms": ms_s,
-            "classes": {str(cl): {"blocks_per_sm": e["blocks_per_sm"], "order": e["order"],
-                                  "tuning_ms": {k: round(v, 1) for k, v in e["timings"].items()}}
-                        for cl, e in plan.items()},
-            "failed": int((sts != 0).sum()),
-            "T_bitwise_equal_to_single_launch": bool(torch.equal(Ts, Tc)) if nfb == 0 else None}
-        out[prec]["schedule"] = "split" if ms_s < ms else "single"
-        out[prec]["best_points_per_s"] = P / min(ms, ms_s) * 1e3
-        b.release(gs)
-        del gs
+        try:
+            plan = tuner.tune_split(b, prec, tune_oms, reps=1, force=True)
+            parts = b.split_parts(it, plan)
+            gs, (Ts, sts, _) = b.graph_split(parts, prec)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record()
+            gs.replay()
+            e1.record()
+            torch.cuda.synchronize()
+            ms_s = e0.elapsed_time(e1)
+            out[prec]["split"] = {
+                "points_per_s": P / ms_s * 1e3, "ms": ms_s,
+                "classes": {str(cl): {"blocks_per_sm": e["blocks_per_sm"], "order": e["order"],
+                                      "tuning_ms": {k: round(v, 1) for k, v in e["timings"].items()}}
+                            for cl, e in plan.items()},
+                "failed": int((sts != 0).sum()),
+                "T_bitwise_equal_to_single_launch": bool(torch.equal(Ts, Tc)) if nfb == 0 else None}
+            out[prec]["schedule"] = "split" if ms_s < ms else "single"
+            out[prec]["best_points_per_s"] = P / min(ms, ms_s) * 1e3
+            b.release(gs)
+            del gs
+        except (RuntimeError, torch.OutOfMemoryError) as e:  # an extra measurement: record, do not abort
+            out[prec]["split"] = {"error": str(e).splitlines()[0][:200]}
     offs = np.cumsum([0] + [o.size * len(w.kpoints) for o, w in zip(oms, ws)])
     errs = []
     for i, w in enumerate(ws):
