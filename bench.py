@@ -498,7 +498,8 @@ def uneven_batch(torch, omega_stride=16, oracle_per_system=2):
         del g
         # Split schedule: one launch per padded-order class, each tuned on its own.
         try:
-            plan = tuner.tune_split(b, prec, tune_oms, reps=1, force=True)
+            split_tuner = BatchTuner(tuner.path, candidates=[(2, "lpt"), (2, "system"), (1, "lpt")])
+            plan = split_tuner.tune_split(b, prec, tune_oms, reps=1, force=True)
             parts = b.split_parts(it, plan)
             gs, (Ts, sts, _) = b.graph_split(parts, prec)
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
