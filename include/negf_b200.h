@@ -284,6 +284,28 @@ int negf_rgf_adjoint_sigma_f64(int n_dev, int n_lead_l, int n_lead_r, int n_laye
                                double* sigma_adj_right, double* t_out, int* status_out, void* workspace,
                                size_t workspace_bytes, void* stream);
 
+/*
+ * negf_rgf_adjoint_sigma_f64 with per-point gradient blocks: grad_onsite is
+ * [batch][n_layers][n][n] and grad_coupling [batch][n_layers-1][n][n], and
+ * point p STORES weight[p] X_ii and weight[p] (X_{i+1,i} + X_{i,i+1}^H) in
+ * its own blocks instead of adding them into shared per-k blocks.  Summing
+ * the points' blocks per k in a fixed order then gives a gradient that is
+ * the same bit for bit from run to run (the FP64 atomic additions of
+ * negf_rgf_adjoint_f64 follow the GPU's scheduling).  Points that fail or
+ * are skipped are not written (the caller zeroes the outputs).  Both
+ * self-energy outputs may be NULL.  Same workspace as negf_rgf_adjoint_f64.
+ */
+int negf_rgf_adjoint_points_f64(int n_dev, int n_lead_l, int n_lead_r, int n_layers, int batch, const double* onsite,
+                                long long onsite_kstride, long long onsite_lstride, const double* coupling,
+                                long long coupling_kstride, long long coupling_lstride, const double* v_left,
+                                long long v_left_kstride, const double* v_right, long long v_right_kstride,
+                                const double* g_left, long long g_left_pstride, const double* g_right,
+                                long long g_right_pstride, const int* k_index, const double* omega,
+                                const double* eta_device, const int* lead_status, const double* weight,
+                                double* grad_onsite, double* grad_coupling, double* sigma_adj_left,
+                                double* sigma_adj_right, double* t_out, int* status_out, void* workspace,
+                                size_t workspace_bytes, void* stream);
+
 /* Workspace bytes negf_sgf_adjoint_f64 needs (0 on a bad size). */
 size_t negf_sgf_adjoint_workspace_bytes(int n_lead, int n_dev);
 
@@ -313,6 +335,21 @@ int negf_sgf_adjoint_f64(int n_lead, int n_dev, int batch, const double* h01, co
                          double tol, int maxiter, double* grad_h00, double* grad_h01, double* grad_h10,
                          double* grad_v, int* iters_out, int* status_out, void* workspace, size_t workspace_bytes,
                          void* stream);
+
+/*
+ * negf_sgf_adjoint_f64 with per-point gradients: grad_h00, grad_h01,
+ * grad_h10 are [batch][n_lead][n_lead] and grad_v [batch][n_lead][n_dev],
+ * and point p STORES its terms in its own slot (summed per k by the caller
+ * in a fixed order for a run-to-run reproducible gradient).  Skipped or
+ * failed points are not written (the caller zeroes the outputs).  Same
+ * workspace as negf_sgf_adjoint_f64.
+ */
+int negf_sgf_adjoint_points_f64(int n_lead, int n_dev, int batch, const double* h01, const double* h10,
+                                long long lead_stride, const double* v, long long v_kstride, const double* g,
+                                long long g_pstride, const double* sigma_adj, const int* k_index,
+                                const int* lead_status, double tol, int maxiter, double* grad_h00, double* grad_h01,
+                                double* grad_h10, double* grad_v, int* iters_out, int* status_out, void* workspace,
+                                size_t workspace_bytes, void* stream);
 
 /*
  * One lead/device/lead system of an uneven batch (negf_batch_transmission).

@@ -86,6 +86,15 @@ _SIGNATURES = {
         _I,
         [_I, _I, _I, _P, _P, _LL, _P, _LL, _P, _LL, _P, _P, _P, _D, _I, _P, _P, _P, _P, _P, _P, _P, _SZ, _P],
     ),
+    "negf_sgf_adjoint_points_f64": (
+        _I,
+        [_I, _I, _I, _P, _P, _LL, _P, _LL, _P, _LL, _P, _P, _P, _D, _I, _P, _P, _P, _P, _P, _P, _P, _SZ, _P],
+    ),
+    "negf_rgf_adjoint_points_f64": (
+        _I,
+        [_I, _I, _I, _I, _I, _P, _LL, _LL, _P, _LL, _LL, _P, _LL, _P, _LL, _P, _LL, _P, _LL, _P, _P, _P, _P, _P,
+         _P, _P, _P, _P, _P, _P, _P, _SZ, _P],
+    ),
     "negf_kavg_f64": (_I, [_P, _I, _I, _P, _P]),
     "negf_heat_current_f64": (_I, [_P, _P, _I, _I, _D, _D, _P, _P]),
     "negf_kmoments_f64": (_I, [_P, _I, _I, _P, _P, _P]),

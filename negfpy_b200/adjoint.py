@@ -30,6 +30,12 @@ import torch
 from . import _lib, engine
 from .hetero import HeteroModel
 
+# Adjoint blocks of each point stored separately and summed per k in a fixed
+# order (negf_rgf_adjoint_points_f64 / negf_sgf_adjoint_points_f64), so that
+# kappa's gradient is the same bit for bit from run to run; False adds them
+# with FP64 atomics instead (rounding-level run-to-run differences).
+DETERMINISTIC = True
+
 HBAR_J_S = 1.054_571_817e-34
 KB_J_K = 1.380_649e-23
 
@@ -93,7 +99,8 @@ class DeviceSolve:
         over the adjoint blocks, in one launch of the adjoint kernel."""
         w = weight.reshape(-1).to(device=self.omega.device, dtype=torch.float64).contiguous()
         T, st, g_on, g_cp = engine.rgf_adjoint(onsite.contiguous(), coupling.contiguous(), self.L, self.vl, self.vr,
-                                               self.g_l, self.g_r, self.omega, self.eta, self.ki, self.lead_status, w)
+                                               self.g_l, self.g_r, self.omega, self.eta, self.ki, self.lead_status, w,
+                                               deterministic=DETERMINISTIC)
         self._check(st)
         return T.reshape(self.W, self.K), g_on, g_cp
 
@@ -268,12 +275,15 @@ def transport_vjp(onsite, coupling, vl, vr, l_d00, l_d01, r_d00, r_d01, pts: Poi
     w = weight.reshape(-1).to(device=pts.omega.device, dtype=torch.float64).contiguous()
     T, st, x_on, x_cp, xs_l, xs_r = engine.rgf_adjoint(onsite.detach().contiguous(), coupling.detach().contiguous(),
                                                        pts.L, vl.detach().contiguous(), vr.detach().contiguous(),
-                                                       g_l, g_r, pts.omega, pts.eta, pts.ki, lst, w, want_sigma=True)
+                                                       g_l, g_r, pts.omega, pts.eta, pts.ki, lst, w, want_sigma=True,
+                                                       deterministic=DETERMINISTIC)
     bad = int((st != 0).sum())
     if bad:
         raise RuntimeError(f"device solve failed at {bad} of {st.numel()} (omega, k) points")
-    al = engine.sgf_adjoint(l_d01.detach(), None, vl.detach(), g_l, xs_l, pts.ki, lst, tol, maxiter)
-    ar = engine.sgf_adjoint(r_d01.detach(), None, vr.detach(), g_r, xs_r, pts.ki, lst, tol, maxiter)
+    al = engine.sgf_adjoint(l_d01.detach(), None, vl.detach(), g_l, xs_l, pts.ki, lst, tol, maxiter,
+                            deterministic=DETERMINISTIC)
+    ar = engine.sgf_adjoint(r_d01.detach(), None, vr.detach(), g_r, xs_r, pts.ki, lst, tol, maxiter,
+                            deterministic=DETERMINISTIC)
     for a in (al, ar):
         nb = int((a["status"] != 0).sum())
         if nb:

@@ -498,7 +498,7 @@ static int rgf_adjoint_common(const char* name, int n_dev, int n_lead_l, int n_l
                               const double* omega, const double* eta_device, const int* lead_status,
                               const double* weight, double* grad_onsite, double* grad_coupling, double* t_out,
                               int* status_out, void* workspace, size_t workspace_bytes, void* stream,
-                              double* sig_adj_l, double* sig_adj_r) {
+                              double* sig_adj_l, double* sig_adj_r, int per_point) {
   if (n_dev <= 0 || n_lead_l <= 0 || n_lead_r <= 0 || n_layers <= 0 || batch < 0)
     return fail2(NEGF_EINVAL, name, "sizes must be positive");
   if (!onsite || !v_left || !v_right || !g_left || !g_right || !omega || !eta_device || !t_out || !weight ||
@@ -549,6 +549,7 @@ static int rgf_adjoint_common(const char* name, int n_dev, int n_lead_l, int n_l
   ga.grad_c = reinterpret_cast<double2*>(grad_coupling ? grad_coupling : grad_onsite);
   ga.sig_adj_l = reinterpret_cast<double2*>(sig_adj_l);
   ga.sig_adj_r = reinterpret_cast<double2*>(sig_adj_r);
+  ga.per_point = per_point;
   cudaStream_t st = as_stream(stream);
   if (cudaMemsetAsync(workspace, 0, sizeof(unsigned int), st) != cudaSuccess)
     return cuda_fail2(name, "counter reset");
@@ -573,7 +574,7 @@ int negf_rgf_adjoint_f64(int n_dev, int n_lead_l, int n_lead_r, int n_layers, in
                             onsite_kstride, onsite_lstride, coupling, coupling_kstride, coupling_lstride, v_left,
                             v_left_kstride, v_right, v_right_kstride, g_left, g_left_pstride, g_right,
                             g_right_pstride, k_index, omega, eta_device, lead_status, weight, grad_onsite,
-                            grad_coupling, t_out, status_out, workspace, workspace_bytes, stream, nullptr, nullptr);
+                            grad_coupling, t_out, status_out, workspace, workspace_bytes, stream, nullptr, nullptr, 0);
 }
 
 int negf_rgf_adjoint_sigma_f64(int n_dev, int n_lead_l, int n_lead_r, int n_layers, int batch, const double* onsite,
@@ -593,7 +594,25 @@ int negf_rgf_adjoint_sigma_f64(int n_dev, int n_lead_l, int n_lead_r, int n_laye
                             v_left_kstride, v_right, v_right_kstride, g_left, g_left_pstride, g_right,
                             g_right_pstride, k_index, omega, eta_device, lead_status, weight, grad_onsite,
                             grad_coupling, t_out, status_out, workspace, workspace_bytes, stream, sigma_adj_left,
-                            sigma_adj_right);
+                            sigma_adj_right, 0);
+}
+
+int negf_rgf_adjoint_points_f64(int n_dev, int n_lead_l, int n_lead_r, int n_layers, int batch, const double* onsite,
+                                long long onsite_kstride, long long onsite_lstride, const double* coupling,
+                                long long coupling_kstride, long long coupling_lstride, const double* v_left,
+                                long long v_left_kstride, const double* v_right, long long v_right_kstride,
+                                const double* g_left, long long g_left_pstride, const double* g_right,
+                                long long g_right_pstride, const int* k_index, const double* omega,
+                                const double* eta_device, const int* lead_status, const double* weight,
+                                double* grad_onsite, double* grad_coupling, double* sigma_adj_left,
+                                double* sigma_adj_right, double* t_out, int* status_out, void* workspace,
+                                size_t workspace_bytes, void* stream) {
+  return rgf_adjoint_common("negf_rgf_adjoint_points_f64", n_dev, n_lead_l, n_lead_r, n_layers, batch, onsite,
+                            onsite_kstride, onsite_lstride, coupling, coupling_kstride, coupling_lstride, v_left,
+                            v_left_kstride, v_right, v_right_kstride, g_left, g_left_pstride, g_right,
+                            g_right_pstride, k_index, omega, eta_device, lead_status, weight, grad_onsite,
+                            grad_coupling, t_out, status_out, workspace, workspace_bytes, stream, sigma_adj_left,
+                            sigma_adj_right, 1);
 }
 
 size_t negf_sgf_adjoint_workspace_bytes(int n_lead, int n_dev) {
@@ -604,25 +623,26 @@ size_t negf_sgf_adjoint_workspace_bytes(int n_lead, int n_dev) {
   return kCounterBytes + negf::sgf_adj_ws_bytes(np, grid);
 }
 
-int negf_sgf_adjoint_f64(int n_lead, int n_dev, int batch, const double* h01, const double* h10,
+static int sgf_adjoint_common(const char* name, int per_point, int n_lead, int n_dev, int batch,
+                              const double* h01, const double* h10,
                          long long lead_stride, const double* v, long long v_kstride, const double* g,
                          long long g_pstride, const double* sigma_adj, const int* k_index, const int* lead_status,
                          double tol, int maxiter, double* grad_h00, double* grad_h01, double* grad_h10,
                          double* grad_v, int* iters_out, int* status_out, void* workspace, size_t workspace_bytes,
                          void* stream) {
   if (n_lead <= 0 || n_dev <= 0 || batch < 0)
-    return fail(NEGF_EINVAL, "negf_sgf_adjoint_f64: sizes must be positive");
+    return fail2(NEGF_EINVAL, name, "sizes must be positive");
   if (!h01 || !v || !g || !sigma_adj || !grad_h00 || !grad_h01 || !grad_v || (h10 && !grad_h10))
-    return fail(NEGF_EINVAL, "negf_sgf_adjoint_f64: null pointer");
+    return fail2(NEGF_EINVAL, name, "null pointer");
   if (lead_stride < 0 || v_kstride < 0 || g_pstride < 0)
-    return fail(NEGF_EINVAL, "negf_sgf_adjoint_f64: negative stride");
-  if (maxiter <= 0 || !(tol > 0.0)) return fail(NEGF_EINVAL, "negf_sgf_adjoint_f64: maxiter and tol must be positive");
-  if (n_lead > 256 || n_dev > 256) return fail(NEGF_EUNSUPPORTED, "negf_sgf_adjoint_f64: block order above 256");
+    return fail2(NEGF_EINVAL, name, "negative stride");
+  if (maxiter <= 0 || !(tol > 0.0)) return fail2(NEGF_EINVAL, name, "maxiter and tol must be positive");
+  if (n_lead > 256 || n_dev > 256) return fail2(NEGF_EUNSUPPORTED, name, "block order above 256");
   const int np = (max3(n_lead, n_dev, 1) + 15) / 16 * 16;
   const int grid = negf::sgf_adj_grid(np);
-  if (grid <= 0) return cuda_fail("negf_sgf_adjoint_f64: occupancy query");
+  if (grid <= 0) return cuda_fail2(name, "occupancy query");
   if (!workspace || workspace_bytes < kCounterBytes + negf::sgf_adj_ws_bytes(np, grid))
-    return fail(NEGF_EINVAL, "negf_sgf_adjoint_f64: workspace missing or too small");
+    return fail2(NEGF_EINVAL, name, "workspace missing or too small");
   if (batch == 0) return 0;
   negf::SgfAdjArgs sa;
   sa.nl = n_lead;
@@ -644,16 +664,39 @@ int negf_sgf_adjoint_f64(int n_lead, int n_dev, int batch, const double* h01, co
   sa.grad_h01 = reinterpret_cast<double2*>(grad_h01);
   sa.grad_h10 = h10 ? reinterpret_cast<double2*>(grad_h10) : nullptr;
   sa.grad_v = reinterpret_cast<double2*>(grad_v);
+  sa.per_point = per_point;
   sa.iters_out = iters_out;
   sa.status_out = status_out;
   sa.counter = reinterpret_cast<unsigned*>(workspace);
   cudaStream_t st = as_stream(stream);
   if (cudaMemsetAsync(workspace, 0, sizeof(unsigned), st) != cudaSuccess)
-    return cuda_fail("negf_sgf_adjoint_f64: counter reset");
+    return cuda_fail2(name, "counter reset");
   if (negf::sgf_adj_launch(sa, np, grid, reinterpret_cast<double2*>(static_cast<char*>(workspace) + kCounterBytes),
                            st) != 0)
-    return cuda_fail("negf_sgf_adjoint_f64");
+    return cuda_fail2(name, "launch");
   return 0;
+}
+
+int negf_sgf_adjoint_f64(int n_lead, int n_dev, int batch, const double* h01, const double* h10,
+                         long long lead_stride, const double* v, long long v_kstride, const double* g,
+                         long long g_pstride, const double* sigma_adj, const int* k_index, const int* lead_status,
+                         double tol, int maxiter, double* grad_h00, double* grad_h01, double* grad_h10,
+                         double* grad_v, int* iters_out, int* status_out, void* workspace, size_t workspace_bytes,
+                         void* stream) {
+  return sgf_adjoint_common("negf_sgf_adjoint_f64", 0, n_lead, n_dev, batch, h01, h10, lead_stride, v, v_kstride, g,
+                            g_pstride, sigma_adj, k_index, lead_status, tol, maxiter, grad_h00, grad_h01, grad_h10,
+                            grad_v, iters_out, status_out, workspace, workspace_bytes, stream);
+}
+
+int negf_sgf_adjoint_points_f64(int n_lead, int n_dev, int batch, const double* h01, const double* h10,
+                                long long lead_stride, const double* v, long long v_kstride, const double* g,
+                                long long g_pstride, const double* sigma_adj, const int* k_index,
+                                const int* lead_status, double tol, int maxiter, double* grad_h00, double* grad_h01,
+                                double* grad_h10, double* grad_v, int* iters_out, int* status_out, void* workspace,
+                                size_t workspace_bytes, void* stream) {
+  return sgf_adjoint_common("negf_sgf_adjoint_points_f64", 1, n_lead, n_dev, batch, h01, h10, lead_stride, v,
+                            v_kstride, g, g_pstride, sigma_adj, k_index, lead_status, tol, maxiter, grad_h00,
+                            grad_h01, grad_h10, grad_v, iters_out, status_out, workspace, workspace_bytes, stream);
 }
 
 int negf_kmoments_f64(const double* t, int n_omega, int n_k, double* t_mean, double* t2_mean, void* stream) {

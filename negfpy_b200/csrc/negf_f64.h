@@ -53,6 +53,7 @@ struct GradArgs {
   double2* grad_c;       // [K][L-1][n][n]  += weight (X_{i+1,i} + X_{i,i+1}^H)
   double2* sig_adj_l;    // [batch][n][n] or nullptr: weight dT/dSigma_L (X_00 + i G Gamma_R G^H)
   double2* sig_adj_r;    // [batch][n][n] or nullptr: weight dT/dSigma_R (X_{L-1,L-1} + i G^H Gamma_L G)
+  int per_point;         // 1: grad_d / grad_c are [batch][..] and each point stores its own blocks
 };
 
 // Adjoint of the surface GF fixed point g = (z - H00 - H01 g H10)^-1 and of
@@ -75,6 +76,7 @@ struct SgfAdjArgs {
   double2* grad_h01;
   double2* grad_h10;       // nullptr when h10 is nullptr
   double2* grad_v;         // [K|1][nl][n]
+  int per_point;           // 1: the four gradients are [batch][..] and each point stores its own
   int* iters_out;
   int* status_out;
   unsigned* counter;

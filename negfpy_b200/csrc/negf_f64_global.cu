@@ -196,6 +196,13 @@ __device__ __forceinline__ void atomic_cadd(double2* dst, double2 v) {
   atomicAdd(&dst->x, v.x);
   atomicAdd(&dst->y, v.y);
 }
+// A point's contribution to a gradient block: added atomically into the
+// shared per-k block, or stored into the point's own block (per-point mode,
+// which the host then sums in a fixed order for a reproducible result).
+__device__ __forceinline__ void grad_put(double2* dst, double2 v, bool own) {
+  if (own) *dst = v;
+  else atomic_cadd(dst, v);
+}
 
 // Per point: T and the weighted adjoint blocks of dT/dD.  With G = A^-1 for
 // A = z - D - Sigma_L - Sigma_R, Y = Gamma_R G_{0,L-1}^H Gamma_L and
@@ -246,8 +253,10 @@ __global__ void __launch_bounds__(kThreads, 2) rgf_grad_f64_kernel(GradArgs ga, 
     const double2* D = a.D + k * a.d_ks;
     const double2* C = a.C + k * a.c_ks;
     const double wgt = ga.weight[p];
-    double2* gdk = ga.grad_d + k * (long long)L * n * n;
-    double2* gck = ga.grad_c + k * (long long)(L > 1 ? L - 1 : 1) * n * n;
+    const bool own = ga.per_point != 0;
+    const long long slot = own ? (long long)p : k;
+    double2* gdk = ga.grad_d + slot * (long long)L * n * n;
+    double2* gck = ga.grad_c + slot * (long long)(L > 1 ? L - 1 : 1) * n * n;
     auto Dl = [&](int l) { return D + (long long)l * a.d_ls; };
     auto load_c = [&](int l) {
       load_pad(Cb, C + (long long)l * a.c_ls, n, n, NP, 0.0);
@@ -357,7 +366,7 @@ __global__ void __launch_bounds__(kThreads, 2) rgf_grad_f64_kernel(GradArgs ga, 
         const int r = (int)(e / NP), c = (int)(e - (long long)r * NP);
         if (r < n && c < n) {
           const double2 v = Xa[e];
-          atomic_cadd(gdk + (long long)i * n * n + r * n + c, make_double2(wgt * v.x, wgt * v.y));
+          grad_put(gdk + (long long)i * n * n + r * n + c, make_double2(wgt * v.x, wgt * v.y), own);
           if (i == 0 && want_l) {
             const double2 zt = Mb[e];
             ga.sig_adj_l[(long long)p * n * n + r * n + c] = make_double2(wgt * (v.x - zt.y), wgt * (v.y + zt.x));
@@ -376,7 +385,7 @@ __global__ void __launch_bounds__(kThreads, 2) rgf_grad_f64_kernel(GradArgs ga, 
           const int r = (int)(e / NP), c = (int)(e - (long long)r * NP);
           if (r < n && c < n) {
             const double2 v = cadd(Xa[e], cconj(Xb[(long long)c * NP + r]));
-            atomic_cadd(gck + (long long)(i - 1) * n * n + r * n + c, make_double2(wgt * v.x, wgt * v.y));
+            grad_put(gck + (long long)(i - 1) * n * n + r * n + c, make_double2(wgt * v.x, wgt * v.y), own);
           }
         }
       }
@@ -481,10 +490,11 @@ __global__ void __launch_bounds__(kThreads, 2) sgf_adjoint_f64_kernel(SgfAdjArgs
     gemm_to<false, false>(Aq, Gb, T2, NP, kl);     // g V^H X      (nl x n)
     gemm_to<false, false>(Bp, T1, Gb, NP, kl);     // X V g        (n x nl)
     {
-      double2* gv = sa.grad_v + k * (sa.v_ks ? (long long)nl * n : 0);
+      const bool own = sa.per_point != 0;
+      double2* gv = sa.grad_v + (own ? (long long)p * nl * n : k * (sa.v_ks ? (long long)nl * n : 0));
       for (long long e = tid; e < M2; e += kThreads) {
         const int r = (int)(e / NP), c = (int)(e - (long long)r * NP);
-        if (r < nl && c < n) atomic_cadd(gv + (long long)r * n + c, cadd(Aq[e], cconj(Bp[(long long)c * NP + r])));
+        if (r < nl && c < n) grad_put(gv + (long long)r * n + c, cadd(Aq[e], cconj(Bp[(long long)c * NP + r])), own);
       }
       __syncthreads();  // Aq and Bp are rewritten next
     }
@@ -534,18 +544,20 @@ __global__ void __launch_bounds__(kThreads, 2) sgf_adjoint_f64_kernel(SgfAdjArgs
       gemm_to<false, false>(T2, Tt, T1, NP, kl);     // H01bar = g H10 H00bar
       gemm_to<false, false>(Aq2, H01b, Gb, NP, kl);  // H01 g
       gemm_to<false, false>(Tt, T1, Aq2, NP, kl);    // H10bar = H00bar H01 g
-      double2* g00 = sa.grad_h00 + k * (long long)nl * nl;
-      double2* g01 = sa.grad_h01 + k * (long long)nl * nl;
-      double2* g10 = sa.grad_h10 ? sa.grad_h10 + k * (long long)nl * nl : nullptr;
+      const bool own = sa.per_point != 0;
+      const long long slot = own ? (long long)p : k;
+      double2* g00 = sa.grad_h00 + slot * nl * nl;
+      double2* g01 = sa.grad_h01 + slot * nl * nl;
+      double2* g10 = sa.grad_h10 ? sa.grad_h10 + slot * nl * nl : nullptr;
       for (long long e = tid; e < M2; e += kThreads) {
         const int r = (int)(e / NP), c = (int)(e - (long long)r * NP);
         if (r < nl && c < nl) {
-          atomic_cadd(g00 + r * nl + c, T1[e]);
+          grad_put(g00 + r * nl + c, T1[e], own);
           if (h10) {
-            atomic_cadd(g01 + r * nl + c, T2[e]);
-            if (g10) atomic_cadd(g10 + r * nl + c, Tt[e]);
+            grad_put(g01 + r * nl + c, T2[e], own);
+            if (g10) grad_put(g10 + r * nl + c, Tt[e], own);
           } else {
-            atomic_cadd(g01 + r * nl + c, cadd(T2[e], cconj(Tt[(long long)c * NP + r])));
+            grad_put(g01 + r * nl + c, cadd(T2[e], cconj(Tt[(long long)c * NP + r])), own);
           }
         }
       }

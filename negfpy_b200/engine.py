@@ -266,10 +266,34 @@ def device_green(onsite: torch.Tensor, coupling: torch.Tensor | None, n_layers: 
     return G, sl, sr, st
 
 
+# Per-point gradient blocks are produced in chunks of at most this many bytes
+# (large chunks keep the persistent adjoint launches full).
+_POINTS_CHUNK_BYTES = 8 << 30
+
+
+def _sum_by_k(dst: torch.Tensor, src: torch.Tensor, kidx: torch.Tensor | None) -> None:
+    """dst[k] += the sum of src[p] over the points p with kidx[p] == k, each
+    k's points summed by one reduction in point order (no atomics), so the
+    result is the same bit for bit from run to run.  kidx None: all into
+    dst[0]."""
+    if src.shape[0] == 0:
+        return
+    if kidx is None or dst.shape[0] == 1:
+        dst[0] += src.sum(0)
+        return
+    kk = kidx.to(torch.int64)
+    order = torch.argsort(kk, stable=True)
+    uniq, counts = torch.unique_consecutive(kk[order], return_counts=True)
+    start = 0
+    for k, c in zip(uniq.tolist(), counts.tolist()):
+        dst[k] += src[order[start:start + c]].sum(0)
+        start += c
+
+
 def rgf_adjoint(onsite: torch.Tensor, coupling: torch.Tensor, n_layers: int, vl: torch.Tensor, vr: torch.Tensor,
                 gl: torch.Tensor, gr: torch.Tensor, omega: torch.Tensor, eta_dev: torch.Tensor,
                 k_index: torch.Tensor, lead_status: torch.Tensor | None, weight: torch.Tensor,
-                stream=None, want_sigma: bool = False):
+                stream=None, want_sigma: bool = False, deterministic: bool = False):
     """Vector-Jacobian product of T with respect to the device blocks.
 
     Layer-resolved blocks ``onsite`` ``[K, L, n, n]`` and ``coupling`` ``[K, L-1, n, n]``
@@ -278,7 +302,12 @@ def rgf_adjoint(onsite: torch.Tensor, coupling: torch.Tensor, n_layers: int, vl:
     over the returned adjoint blocks (``negf_rgf_adjoint_f64``).  With
     ``want_sigma`` it also returns the per-point weighted adjoints of the two
     contact self-energies ``[P, n, n]`` (``negf_rgf_adjoint_sigma_f64``), the
-    input of ``sgf_adjoint``."""
+    input of ``sgf_adjoint``.
+
+    ``deterministic``: the points store their blocks separately
+    (``negf_rgf_adjoint_points_f64``, in chunks of at most 8 GiB) and the
+    blocks are summed per k in a fixed order, so the gradient is the same
+    bit for bit from run to run (the default adds them with FP64 atomics)."""
     lib = _lib.load()
     dev = _dev()
     K, L, n, _ = onsite.shape
@@ -309,6 +338,31 @@ def rgf_adjoint(onsite: torch.Tensor, coupling: torch.Tensor, n_layers: int, vl:
               _lib.ptr(k_index), _lib.ptr(omega), _lib.ptr(eta_dev), _lib.ptr(lead_status), _lib.ptr(weight),
               _lib.ptr(g_on), _lib.ptr(g_cp if L > 1 else None))
     tail = (_lib.ptr(T), _lib.ptr(st), _lib.ptr(ws), ws.numel(), _lib.stream_handle(stream))
+    if deterministic:
+        weight = weight.to(device=dev, dtype=RDT).contiguous()
+        lst = None if lead_status is None else lead_status.to(device=dev, dtype=torch.int32).contiguous()
+        chunk = max(1, min(P, _POINTS_CHUNK_BYTES // ((2 * L - 1) * n * n * 16)))
+        pp_on = torch.empty((chunk, L, n, n), dtype=CDT, device=dev)
+        pp_cp = torch.empty((chunk, max(L - 1, 1), n, n), dtype=CDT, device=dev)
+        for a in range(0, P, chunk):
+            b = min(P, a + chunk)
+            c = b - a
+            pp_on[:c].zero_()
+            pp_cp[:c].zero_()
+            sl = slice(a, b)
+            rc = lib.negf_rgf_adjoint_points_f64(
+                n, nl, nr, L, c, _lib.ptr(onsite), L * n * n, n * n, _lib.ptr(cp), (L - 1) * n * n, n * n,
+                _lib.ptr(vl), vl_ks, _lib.ptr(vr), vr_ks, _lib.ptr(gl[sl]), nl * nl, _lib.ptr(gr[sl]), nr * nr,
+                _lib.ptr(k_index[sl]), _lib.ptr(omega[sl]), _lib.ptr(eta_dev[sl]),
+                _lib.ptr(None if lst is None else lst[sl]), _lib.ptr(weight[sl]), _lib.ptr(pp_on),
+                _lib.ptr(pp_cp if L > 1 else None), _lib.ptr(None if xs_l is None else xs_l[sl]),
+                _lib.ptr(None if xs_r is None else xs_r[sl]), _lib.ptr(T[sl]), _lib.ptr(st[sl]), _lib.ptr(ws),
+                ws.numel(), _lib.stream_handle(stream))
+            _lib.check(rc, "negf_rgf_adjoint_points_f64")
+            _sum_by_k(g_on, pp_on[:c], k_index[sl])
+            if L > 1:
+                _sum_by_k(g_cp, pp_cp[:c], k_index[sl])
+        return (T, st, g_on, g_cp, xs_l, xs_r) if want_sigma else (T, st, g_on, g_cp)
     if want_sigma:
         rc = lib.negf_rgf_adjoint_sigma_f64(*common, _lib.ptr(xs_l), _lib.ptr(xs_r), *tail)
         _lib.check(rc, "negf_rgf_adjoint_sigma_f64")
@@ -320,7 +374,7 @@ def rgf_adjoint(onsite: torch.Tensor, coupling: torch.Tensor, n_layers: int, vl:
 
 def sgf_adjoint(d01: torch.Tensor, d10: torch.Tensor | None, v: torch.Tensor, g: torch.Tensor,
                 sigma_adj: torch.Tensor, k_index: torch.Tensor | None, lead_status: torch.Tensor | None = None,
-                tol: float = 1e-12, maxiter: int = 200, stream=None) -> dict:
+                tol: float = 1e-12, maxiter: int = 200, stream=None, deterministic: bool = False) -> dict:
     """Adjoint of the lead surface GF and of Sigma = V g V^H (``negf_sgf_adjoint_f64``).
 
     ``d01``/``d10`` ``[K, nl, nl]`` (d10 None: d01^H), ``v`` ``[K|1, n, nl]``,
@@ -329,7 +383,9 @@ def sgf_adjoint(d01: torch.Tensor, d10: torch.Tensor | None, v: torch.Tensor, g:
     Returns the per-k adjoint blocks (dT = 2 Re Tr[dH X]) ``h00``, ``h01``,
     ``h10`` (None when d10 is None: its part is folded into ``h01``) of shape
     ``[K, nl, nl]``, ``v`` of shape ``[K|1, nl, n]``, and per-point
-    ``iters``/``status``."""
+    ``iters``/``status``.  ``deterministic``: per-point terms
+    (``negf_sgf_adjoint_points_f64``) summed per k in a fixed order, the same
+    bit for bit from run to run (the default adds them with FP64 atomics)."""
     lib = _lib.load()
     dev = _dev()
     if d01.dim() == 2:
@@ -353,6 +409,38 @@ def sgf_adjoint(d01: torch.Tensor, d10: torch.Tensor | None, v: torch.Tensor, g:
     ws = _workspace(need, dev, "sgf_adjoint")
     if k_index is not None:
         k_index = k_index.to(device=dev, dtype=torch.int32).contiguous()
+    if deterministic:
+        d01c = d01.contiguous()
+        d10c = None if d10 is None else d10.contiguous()
+        vc, gc, xc = v.contiguous(), g.contiguous(), sigma_adj.contiguous()
+        lst = None if lead_status is None else lead_status.to(device=dev, dtype=torch.int32).contiguous()
+        per = (3 * nl * nl + nl * n) * 16
+        chunk = max(1, min(P, _POINTS_CHUNK_BYTES // per))
+        p00 = torch.empty((chunk, nl, nl), dtype=CDT, device=dev)
+        p01 = torch.empty((chunk, nl, nl), dtype=CDT, device=dev)
+        p10 = None if d10 is None else torch.empty((chunk, nl, nl), dtype=CDT, device=dev)
+        pv = torch.empty((chunk, nl, n), dtype=CDT, device=dev)
+        for a in range(0, P, chunk):
+            b = min(P, a + chunk)
+            c = b - a
+            sl = slice(a, b)
+            for t in (p00, p01, p10, pv):
+                if t is not None:
+                    t[:c].zero_()
+            rc = lib.negf_sgf_adjoint_points_f64(
+                nl, n, c, _lib.ptr(d01c), _lib.ptr(d10c), nl * nl if K > 1 else 0, _lib.ptr(vc),
+                n * nl if v.shape[0] > 1 else 0, _lib.ptr(gc[sl]), nl * nl, _lib.ptr(xc[sl]),
+                _lib.ptr(None if k_index is None else k_index[sl]), _lib.ptr(None if lst is None else lst[sl]),
+                float(tol), int(maxiter), _lib.ptr(p00), _lib.ptr(p01), _lib.ptr(p10), _lib.ptr(pv),
+                _lib.ptr(iters[sl]), _lib.ptr(status[sl]), _lib.ptr(ws), ws.numel(), _lib.stream_handle(stream))
+            _lib.check(rc, "negf_sgf_adjoint_points_f64")
+            ks = None if k_index is None else k_index[sl]
+            _sum_by_k(gh00, p00[:c], ks)
+            _sum_by_k(gh01, p01[:c], ks)
+            if gh10 is not None:
+                _sum_by_k(gh10, p10[:c], ks)
+            _sum_by_k(gv, pv[:c], ks)
+        return out
     rc = lib.negf_sgf_adjoint_f64(nl, n, P, _lib.ptr(d01.contiguous()), _lib.ptr(None if d10 is None else
                                                                                 d10.contiguous()),
                                   nl * nl if K > 1 else 0, _lib.ptr(v.contiguous()), n * nl if v.shape[0] > 1 else 0,
