@@ -95,3 +95,30 @@ def test_order_classes_and_split_parts():
     assert list(sub32.perm.numpy()) == [102, 104, 100, 106]  # lpt inside the class: costs 3, 1.5, 1, 0.5
     assert list(parts[2][2].perm.numpy()) == [103, 105]        # "system": the given order
     assert sum(int(p[2].system.numel()) for p in parts) == 7
+
+
+def test_sum_by_k_groups_points_in_order():
+    """The per-k reduction of per-point adjoint blocks (host side of the
+    reproducible gradients): each k gets the sum of exactly its points, all
+    into slot 0 when there is one slot or no k index, and a repeat gives the
+    same bits."""
+    import torch
+
+    from negfpy_b200.engine import _sum_by_k
+
+    gen = torch.Generator().manual_seed(5)
+    src = torch.randn((9, 2, 3), dtype=torch.complex128, generator=gen)
+    kidx = torch.tensor([2, 0, 2, 1, 0, 2, 1, 1, 0], dtype=torch.int32)
+    dst = torch.zeros((3, 2, 3), dtype=torch.complex128)
+    _sum_by_k(dst, src, kidx)
+    for k in range(3):
+        assert torch.allclose(dst[k], src[kidx == k].sum(0), rtol=0, atol=1e-14)
+    again = torch.zeros_like(dst)
+    _sum_by_k(again, src, kidx)
+    assert torch.equal(again, dst)
+    one = torch.zeros((1, 2, 3), dtype=torch.complex128)
+    _sum_by_k(one, src, kidx)
+    assert torch.allclose(one[0], src.sum(0), rtol=0, atol=1e-14)
+    none = torch.zeros((1, 2, 3), dtype=torch.complex128)
+    _sum_by_k(none, src, None)
+    assert torch.equal(none, one)
