@@ -49,3 +49,16 @@ def test_fp32_product_path_switch_without_gpu():
     assert lib.negf_set_fp32_product_path(0, 0) == -1  # NEGF_EINVAL
     assert lib.negf_set_fp32_product_path(48, 2) == -1
     lib.negf_set_fp32_product_path(160, -1)
+
+
+def test_product_path_tuner_keeps_mma_sync_above_order_128(tmp_path):
+    """Orders above 128 have only the mma.sync tiling: the tuner sets it
+    without timing anything (no GPU needed)."""
+    from types import SimpleNamespace
+
+    from negfpy_b200.autotune import ProductPathTuner
+
+    system = SimpleNamespace(n=160, nl=160, nr=160, n_layers=4)
+    e = ProductPathTuner(tmp_path / "tune.json").tune(system, None, None, None)
+    assert e["path"] == 0 and e["order"] == "mma.sync" and e["timings"] == {}
+    assert _lib.load().negf_set_fp32_product_path(160, -1) == 0
