@@ -62,3 +62,20 @@ def test_product_path_tuner_keeps_mma_sync_above_order_128(tmp_path):
     e = ProductPathTuner(tmp_path / "tune.json").tune(system, None, None, None)
     assert e["path"] == 0 and e["order"] == "mma.sync" and e["timings"] == {}
     assert _lib.load().negf_set_fp32_product_path(160, -1) == 0
+
+
+def test_per_point_adjoint_entries_validate_without_gpu():
+    """The per-point adjoint entries reject bad sizes and missing pointers
+    before touching a device, with messages naming the entry point."""
+    lib = _lib.load()
+    z = [None] * 40
+    # negf_sgf_adjoint_points_f64(n_lead=0, ...)
+    rc = lib.negf_sgf_adjoint_points_f64(0, 4, 1, None, None, 0, None, 0, None, 0, None, None, None, 1e-12, 10,
+                                         *z[:6], None, 0, None)
+    assert rc == -1 and lib.negf_last_error().decode().startswith("negf_sgf_adjoint_points_f64")
+    # negf_rgf_adjoint_points_f64 with every pointer missing
+    rc = lib.negf_rgf_adjoint_points_f64(4, 4, 4, 2, 1, None, 0, 0, None, 0, 0, None, 0, None, 0, None, 0, None, 0,
+                                         *z[:11], None, 0, None)
+    assert rc == -1
+    msg = lib.negf_last_error().decode()
+    assert msg.startswith("negf_rgf_adjoint_points_f64") and "null pointer" in msg
